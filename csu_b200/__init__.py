@@ -1,0 +1,236 @@
+"""csu_b200 -- B200 engine for the residual-and-update path of CSU (2D unstructured finite volumes).
+
+Python view of the C ABI declared in include/csu_gpu.h. The native library is required: importing
+works without it (so the CPU-side tests can check the build), but every call that needs it raises
+`NativeLibraryMissing` instead of falling back to anything else.
+
+    case = Case.load("/tmp/wedge/")            # input.dat + mesh.su2 (+ restart.csv), like solverInit
+    eng = Engine(case)                          # device layout + state, like solverMalloc/InitDomain
+    hist = eng.iterate(100)                     # solverSolve iterations: res[Nvar], Cx_p, Cx_v, Cy_p, Cy_v
+    U = eng.get_state()                         # [Nvar, Nelem] in the reference's cell order
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libcsu_b200.so")
+
+CSU_OK = 0
+ERRORS = {
+    1: "CSU_ERR_INPUT", 2: "CSU_ERR_IO", 3: "CSU_ERR_OOM", 4: "CSU_ERR_NONFINITE", 5: "CSU_ERR_DIVERGED",
+    6: "CSU_ERR_CANCELLED", 7: "CSU_ERR_CUDA", 8: "CSU_ERR_UNSUPPORTED", 9: "CSU_ERR_STATE",
+    10: "CSU_ERR_NO_DEVICE",
+}
+DUMP = {"P": 1, "GHOST_P": 2, "GRAD": 3, "PHI": 4, "FACEFLUX": 5, "R": 6, "D": 7, "DTL": 8, "DW": 9, "BLOCKS": 10}
+FLUX = {"ROE": 0, "AUSM": 1, "AUSMDV": 2, "AUSMpup": 3, "AUSMpup2": 4}
+BC = {"symmetry": 0, "inlet": 1, "outlet": 2, "wall": 3, "wallT": 4}
+
+
+class NativeLibraryMissing(RuntimeError):
+    pass
+
+
+class CsuError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__("%s: %s" % (ERRORS.get(status, status), msg))
+        self.status = status
+
+
+class Config(C.Structure):
+    _fields_ = [(n, C.c_int) for n in (
+        "nvar", "order", "flux", "stages", "time_scheme", "n_linear", "dt_local", "dt_local_n", "laminar", "sa",
+        "sa_cc", "sst", "sst_trans", "axisymmetric", "turb1order", "visc_blazek", "tp", "limiter_type", "tube")] + [
+        (n, C.c_double) for n in ("limiter_k", "cfl", "w_imp", "r_lim", "p_out", "t_wall", "sref", "turb_ratio",
+                                  "e_fix", "pr", "pr_t", "gamma", "gas_r")] + [
+        ("pin", C.c_double * 7), ("uin", C.c_double * 6), ("mach_inf", C.c_double), ("inlet_p", C.c_double),
+        ("inlet_t", C.c_double), ("sst_l", C.c_double), ("k_factor", C.c_double), ("o_factor", C.c_double),
+        ("o_wall_factor", C.c_double)]
+
+
+class MeshDesc(C.Structure):
+    _fields_ = [("n_points", C.c_int), ("xy", C.c_void_p), ("n_cells", C.c_int), ("cell_npts", C.c_void_p),
+                ("cell_nodes", C.c_void_p), ("n_faces", C.c_int), ("con", C.c_void_p), ("cell_nint", C.c_void_p),
+                ("cell_faces", C.c_void_p), ("cell_nei", C.c_void_p), ("n_markers", C.c_int),
+                ("marker_nbf", C.c_void_p), ("marker_flag", C.c_void_p), ("n_bfaces", C.c_int),
+                ("bface", C.c_void_p), ("wall_dist", C.c_void_p)]
+
+
+_lib = None
+
+
+def lib():
+    """The loaded native library (raises NativeLibraryMissing when it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise NativeLibraryMissing("%s is missing: run `python csu_b200/build.py`" % LIB_PATH)
+        L = C.CDLL(LIB_PATH)
+        vp, ip, dp = C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_double)
+        L.csu_last_error.restype = C.c_char_p
+        L.csu_strerror.restype = C.c_char_p
+        L.csu_case_load.argtypes = [C.c_char_p, C.POINTER(vp)]
+        L.csu_case_load_mem.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, C.POINTER(vp)]
+        L.csu_case_mesh.argtypes = [vp, C.POINTER(MeshDesc)]
+        L.csu_case_config.argtypes = [vp, C.POINTER(Config)]
+        L.csu_case_initial_state.argtypes = [vp, vp]
+        L.csu_case_get_int.argtypes = [vp, C.c_char_p, ip]
+        L.csu_case_get_double.argtypes = [vp, C.c_char_p, dp]
+        L.csu_case_marker_name.argtypes = [vp, C.c_int, C.c_char_p, C.c_int]
+        L.csu_case_free.argtypes = [vp]
+        L.csu_case_free.restype = None
+        L.csu_create.argtypes = [C.POINTER(MeshDesc), C.POINTER(Config), C.POINTER(vp)]
+        L.csu_destroy.argtypes = [vp]
+        L.csu_destroy.restype = None
+        L.csu_set_state.argtypes = [vp, vp]
+        L.csu_get_state.argtypes = [vp, vp]
+        L.csu_residual.argtypes = [vp, vp]
+        L.csu_iterate.argtypes = [vp, C.c_int, C.c_int, vp]
+        L.csu_tube_run.argtypes = [vp, C.c_double, ip, dp]
+        L.csu_dump.argtypes = [vp, C.c_int, vp]
+        L.csu_stats.argtypes = [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
+        _lib = L
+    return _lib
+
+
+def _check(st):
+    if st != CSU_OK:
+        raise CsuError(st, lib().csu_last_error().decode(errors="replace"))
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _arr(ptr, n, ctype, dtype):
+    if not ptr or n == 0:
+        return np.zeros(0, dtype)
+    return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(ctype)), shape=(n,)).astype(dtype, copy=True)
+
+
+class Case:
+    """A case folder read by the host C front end (input.dat keywords, SU2 mesh, initial state)."""
+
+    def __init__(self, handle):
+        self._h = C.c_void_p(handle)
+        d = MeshDesc()
+        _check(lib().csu_case_mesh(self._h, C.byref(d)))
+        self.desc = d
+        cfg = Config()
+        _check(lib().csu_case_config(self._h, C.byref(cfg)))
+        self.config = cfg
+        nc, nf, nb = d.n_cells, d.n_faces, d.n_bfaces
+        self.n_cells, self.n_faces, self.n_bfaces, self.n_points = nc, nf, nb, d.n_points
+        self.nvar = cfg.nvar
+        self.xy = _arr(d.xy, 2 * d.n_points, C.c_double, np.float64).reshape(-1, 2)
+        self.cell_npts = _arr(d.cell_npts, nc, C.c_int, np.int32)
+        self.cell_nodes = _arr(d.cell_nodes, 4 * nc, C.c_int, np.int32).reshape(-1, 4)
+        self.con = _arr(d.con, 4 * nf, C.c_int, np.int32).reshape(-1, 4)
+        self.cell_nint = _arr(d.cell_nint, nc, C.c_int, np.int32)
+        self.cell_faces = _arr(d.cell_faces, 4 * nc, C.c_int, np.int32).reshape(-1, 4)
+        self.cell_nei = _arr(d.cell_nei, 4 * nc, C.c_int, np.int32).reshape(-1, 4)
+        self.marker_nbf = _arr(d.marker_nbf, d.n_markers, C.c_int, np.int32)
+        self.marker_flag = _arr(d.marker_flag, d.n_markers, C.c_int, np.int32)
+        self.bface = _arr(d.bface, 3 * nb, C.c_int, np.int32).reshape(-1, 3)
+        self.wall_dist = _arr(d.wall_dist, nc, C.c_double, np.float64) if d.wall_dist else None
+
+    @classmethod
+    def load(cls, wd):
+        if not wd.endswith("/"):
+            wd += "/"
+        h = C.c_void_p()
+        _check(lib().csu_case_load(wd.encode(), C.byref(h)))
+        return cls(h.value)
+
+    @classmethod
+    def from_text(cls, input_dat, mesh_su2, restart_csv=None):
+        h = C.c_void_p()
+        _check(lib().csu_case_load_mem(input_dat.encode(), mesh_su2.encode(),
+                                       restart_csv.encode() if restart_csv else None, C.byref(h)))
+        return cls(h.value)
+
+    def initial_state(self):
+        U = np.zeros(self.nvar * self.n_cells)
+        _check(lib().csu_case_initial_state(self._h, _ptr(U)))
+        return U.reshape(self.nvar, self.n_cells)
+
+    def get_int(self, key):
+        v = C.c_int()
+        _check(lib().csu_case_get_int(self._h, key.encode(), C.byref(v)))
+        return v.value
+
+    def get_double(self, key):
+        v = C.c_double()
+        _check(lib().csu_case_get_double(self._h, key.encode(), C.byref(v)))
+        return v.value
+
+    def marker_name(self, m):
+        buf = C.create_string_buffer(64)
+        _check(lib().csu_case_marker_name(self._h, m, buf, 64))
+        return buf.value.decode()
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.csu_case_free(self._h)
+            self._h = None
+
+
+class Engine:
+    """Device engine of one solve (a csu_ctx)."""
+
+    def __init__(self, case, config=None, state=None):
+        self.case = case
+        self.config = config if config is not None else case.config
+        self.nvar = self.config.nvar
+        self.n_cells = case.n_cells
+        h = C.c_void_p()
+        _check(lib().csu_create(C.byref(case.desc), C.byref(self.config), C.byref(h)))
+        self._h = h
+        self.set_state(case.initial_state() if state is None else state)
+
+    def set_state(self, U):
+        U = np.ascontiguousarray(U, dtype=np.float64).reshape(self.nvar, self.n_cells)
+        _check(lib().csu_set_state(self._h, _ptr(U)))
+
+    def get_state(self):
+        U = np.zeros((self.nvar, self.n_cells))
+        _check(lib().csu_get_state(self._h, _ptr(U)))
+        return U
+
+    def residual(self):
+        R = np.zeros((self.nvar, self.n_cells))
+        _check(lib().csu_residual(self._h, _ptr(R)))
+        return R
+
+    def iterate(self, n, it0=0):
+        hist = np.zeros((max(n, 1), self.nvar + 4))
+        _check(lib().csu_iterate(self._h, n, it0, _ptr(hist)))
+        return hist[:n]
+
+    def tube_run(self, tmax):
+        steps, t = C.c_int(), C.c_double()
+        _check(lib().csu_tube_run(self._h, tmax, C.byref(steps), C.byref(t)))
+        return steps.value, t.value
+
+    def dump(self, what):
+        nc, nv, nf, nb = self.n_cells, self.nvar, self.case.n_faces, self.case.n_bfaces
+        shapes = {"P": (nc, nv + 1), "GHOST_P": (nb, nv + 1), "GRAD": (2, nv, nc), "PHI": (nv, nc),
+                  "FACEFLUX": (nv, nf), "R": (nv, nc), "D": (nc,), "DTL": (nc,), "DW": (nv, nc),
+                  "BLOCKS": (nc, 4, nv, nv)}
+        out = np.zeros(shapes[what])
+        _check(lib().csu_dump(self._h, DUMP[what], _ptr(out)))
+        return out
+
+    def stats(self):
+        a, b = C.c_longlong(), C.c_longlong()
+        _check(lib().csu_stats(self._h, C.byref(a), C.byref(b)))
+        return {"kernel_launches": a.value, "device_bytes": b.value}
+
+    def close(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.csu_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()

@@ -1,0 +1,794 @@
+// capi.cu -- the extern "C" entry points of include/csu_gpu.h: device context, data upload, the per-iteration
+// launch sequences and their CUDA-graph replay.
+#include <cuda_runtime.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <math.h>
+#include <vector>
+#include "csu_gpu.h"
+#include "kernels.cuh"
+
+extern "C" {
+#include "../host/layout.h"
+void csu_set_error(const char* fmt, ...);
+}
+
+using namespace csu;
+
+namespace {
+
+struct Arena {
+    char* base = nullptr;
+    size_t size = 0, used = 0;
+};
+
+// RK stage coefficients of solverStepRK (solver.c:788-840)
+const double RK1[1] = {1.0};
+const double RK3[3] = {0.1481, 0.4, 1.0};
+const double RK4[4] = {0.0833, 0.2069, 0.4265, 1.0};
+const double RK5[5] = {0.0533, 0.1263, 0.2375, 0.4414, 1.0};
+
+} // namespace
+
+struct csu_ctx {
+    int model = 0, nv = 4;
+    csu_config cfg;
+    csu_layout L;
+    Prm prm;
+    Mesh mesh;
+    State st;
+    Arena arena;
+    void* state_base = nullptr;
+    size_t state_bytes = 0;
+    int* d_wall_rank = nullptr;
+    int nwall = 0;
+    cudaStream_t stream = nullptr;
+    int prepared = 0;
+    int xcur = 0;
+    long long launches = 0;
+    int hist_cap = 0;
+    int gb_c = 0, gb_fi = 0, gb_fb = 0;
+    const double* rk = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    int graph_iters = 0;
+    int have_debug = 0;
+};
+
+static int cuda_fail(cudaError_t e, const char* what)
+{
+    csu_set_error("%s: %s", what, cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? CSU_ERR_OOM : CSU_ERR_CUDA;
+}
+
+#define CK(call)                                                                                                   \
+    do {                                                                                                           \
+        cudaError_t e_ = (call);                                                                                   \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call);                                                        \
+    } while (0)
+
+template <typename T>
+static T* carve(Arena& a, size_t count)
+{
+    size_t bytes = (count * sizeof(T) + 255) & ~size_t(255);
+    if (a.base == nullptr) {
+        a.size += bytes; // sizing pass
+        return nullptr;
+    }
+    T* p = reinterpret_cast<T*>(a.base + a.used);
+    a.used += bytes;
+    return p;
+}
+
+// Lays out every device array of a context in one allocation (first pass sizes, second pass carves).
+static void plan(csu_ctx* x, Arena& a)
+{
+    const int nc = x->L.nc, nf = x->L.nf, nb = x->L.nb, nv = x->nv, nx = nv - 4;
+    const size_t c4 = (size_t)4 * nc;
+    Mesh& m = x->mesh;
+    State& s = x->st;
+    m.npts = carve<int>(a, nc);
+    m.nint = carve<int>(a, nc);
+    m.nslot = carve<int>(a, nc);
+    m.nei = carve<int>(a, c4);
+    m.wx = carve<double>(a, c4);
+    m.wy = carve<double>(a, c4);
+    m.ex = carve<double>(a, c4);
+    m.ey = carve<double>(a, c4);
+    m.fslot = carve<int>(a, c4);
+    m.omega = carve<double>(a, nc);
+    m.sxh = carve<double>(a, nc);
+    m.syh = carve<double>(a, nc);
+    m.wall_d = x->L.wall_d ? carve<double>(a, nc) : nullptr;
+    m.dslat = carve<double>(a, nc);
+    m.fe = carve<int2>(a, nf);
+    m.fn = carve<double2>(a, nf);
+    m.fds = carve<double>(a, nf);
+    m.r0 = carve<double2>(a, nf);
+    m.r1 = carve<double2>(a, nf);
+    m.bown = carve<int>(a, nb);
+    m.bflag = carve<int>(a, nb);
+    m.bold = carve<int>(a, nb);
+    m.bn = carve<double2>(a, nb);
+    m.bds = carve<double>(a, nb);
+    x->d_wall_rank = carve<int>(a, nb);
+
+    s.U4 = carve<double4>(a, nc);
+    s.Ux = carve<double>(a, (size_t)nx * nc);
+    s.W4 = carve<double4>(a, nc);
+    s.WT = carve<double>(a, nc);
+    s.Wx = carve<double>(a, (size_t)nx * nc);
+    s.G4x = carve<double4>(a, nc);
+    s.G4y = carve<double4>(a, nc);
+    s.PH4 = carve<double4>(a, nc);
+    s.Gxx = carve<double>(a, (size_t)nx * nc);
+    s.Gxy = carve<double>(a, (size_t)nx * nc);
+    s.PHx = carve<double>(a, (size_t)nx * nc);
+    s.F4 = carve<double4>(a, (size_t)nf + nb);
+    s.Fx = carve<double>(a, (size_t)nx * (nf + nb));
+    s.R4 = carve<double4>(a, nc);
+    s.Rx = carve<double>(a, (size_t)nx * nc);
+    s.dtl = carve<double>(a, nc);
+    s.dpart = carve<double>(a, nc);
+    int implicit = x->cfg.time_scheme != CSU_TS_RK;
+    for (int k = 0; k < 2; k++) {
+        s.X4[k] = implicit ? carve<double4>(a, nc) : nullptr;
+        s.Xx[k] = implicit ? carve<double>(a, (size_t)nx * nc) : nullptr;
+    }
+    s.blocks = x->cfg.time_scheme == CSU_TS_DPLUR ? carve<double>(a, c4 * nv * nv) : nullptr;
+    s.part = carve<double>(a, (size_t)((nc + BLOCK - 1) / BLOCK) * nv);
+    s.bcoef = carve<double>(a, (size_t)4 * (nb > 0 ? nb : 1));
+    s.sc = carve<Scalars>(a, 1);
+    s.dbg_ghost = carve<double>(a, (size_t)(nb > 0 ? nb : 1) * (nv + 1));
+}
+
+static int upload_mesh(csu_ctx* x)
+{
+    const csu_layout& L = x->L;
+    const int nc = L.nc, nf = L.nf, nb = L.nb;
+    const size_t c4 = (size_t)4 * nc;
+    Mesh& m = x->mesh;
+    auto up = [&](const void* dst, const void* src, size_t bytes) -> cudaError_t {
+        if (bytes == 0) return cudaSuccess;
+        return cudaMemcpy(const_cast<void*>(dst), src, bytes, cudaMemcpyHostToDevice);
+    };
+    std::vector<int2> fe(nf);
+    std::vector<double2> fn(nf), r0(nf), r1(nf), bn(nb);
+    for (int f = 0; f < nf; f++) {
+        fe[f] = make_int2(L.fe0[f], L.fe1[f]);
+        fn[f] = make_double2(L.fdsx[f], L.fdsy[f]);
+        r0[f] = make_double2(L.r0x[f], L.r0y[f]);
+        r1[f] = make_double2(L.r1x[f], L.r1y[f]);
+    }
+    for (int b = 0; b < nb; b++) bn[b] = make_double2(L.bdsx[b], L.bdsy[b]);
+    // walls in reference order (solverCalcCoeff3 sums over wall markers, marker-major)
+    std::vector<int> rank(nb > 0 ? nb : 1, -1);
+    {
+        std::vector<int> by_old(nb, -1);
+        for (int b = 0; b < nb; b++) by_old[L.bold[b]] = b;
+        int r = 0;
+        for (int o = 0; o < nb; o++) {
+            int b = by_old[o];
+            if (L.bflag[b] == CSU_BC_WALL || L.bflag[b] == CSU_BC_WALLT) rank[b] = r++;
+        }
+        x->nwall = r;
+    }
+    CK(up(m.npts, L.npts, sizeof(int) * nc));
+    CK(up(m.nint, L.nint, sizeof(int) * nc));
+    CK(up(m.nslot, L.nslot, sizeof(int) * nc));
+    CK(up(m.nei, L.nei, sizeof(int) * c4));
+    CK(up(m.wx, L.wx, sizeof(double) * c4));
+    CK(up(m.wy, L.wy, sizeof(double) * c4));
+    CK(up(m.ex, L.ex, sizeof(double) * c4));
+    CK(up(m.ey, L.ey, sizeof(double) * c4));
+    CK(up(m.fslot, L.fslot, sizeof(int) * c4));
+    CK(up(m.omega, L.omega, sizeof(double) * nc));
+    CK(up(m.sxh, L.sxh, sizeof(double) * nc));
+    CK(up(m.syh, L.syh, sizeof(double) * nc));
+    if (m.wall_d) CK(up(m.wall_d, L.wall_d, sizeof(double) * nc));
+    CK(up(m.dslat, L.dslat, sizeof(double) * nc));
+    CK(up(m.fe, fe.data(), sizeof(int2) * nf));
+    CK(up(m.fn, fn.data(), sizeof(double2) * nf));
+    CK(up(m.fds, L.fds, sizeof(double) * nf));
+    CK(up(m.r0, r0.data(), sizeof(double2) * nf));
+    CK(up(m.r1, r1.data(), sizeof(double2) * nf));
+    CK(up(m.bown, L.bown, sizeof(int) * nb));
+    CK(up(m.bflag, L.bflag, sizeof(int) * nb));
+    CK(up(m.bold, L.bold, sizeof(int) * nb));
+    CK(up(m.bn, bn.data(), sizeof(double2) * nb));
+    CK(up(m.bds, L.bds, sizeof(double) * nb));
+    CK(up(x->d_wall_rank, rank.data(), sizeof(int) * nb));
+    return CSU_OK;
+}
+
+static void fill_params(csu_ctx* x)
+{
+    const csu_config& c = x->cfg;
+    Prm& p = x->prm;
+    memset(&p, 0, sizeof(p));
+    p.gas.gamma = c.gamma;
+    p.gas.R = c.gas_r;
+    p.gas.Cp = c.gamma * c.gas_r / (c.gamma - 1); // gaspropInit (gasprop.c:14-37)
+    p.gas.Cv = p.gas.Cp - c.gas_r;
+    p.gas.tp = c.tp;
+    p.nc = x->L.nc;
+    p.nf = x->L.nf;
+    p.nb = x->L.nb;
+    p.order = c.order;
+    p.scheme = c.flux;
+    p.laminar = c.laminar;
+    p.sa = c.sa;
+    p.sst = c.sst;
+    p.axi = c.axisymmetric;
+    p.turb1order = c.turb1order;
+    p.limiter_type = c.limiter_type;
+    p.stages = c.stages;
+    p.dt_local_n = c.dt_local_n;
+    p.tube = c.tube;
+    p.n_linear = c.n_linear;
+    p.lim_k = c.limiter_k;
+    p.vol_max = x->L.vol_max;
+    p.e_fix = c.e_fix;
+    p.r_lim = c.r_lim;
+    p.p_out = c.p_out;
+    p.t_wall = c.t_wall;
+    p.pr = c.pr;
+    p.pr_t = c.pr_t;
+    p.w_imp = c.w_imp;
+    p.cfl = c.cfl;
+    p.sigma = 0.5 * c.stages;
+    p.mach_inf = c.mach_inf;
+    p.sref = c.sref;
+    for (int k = 0; k < 7; k++) p.pin[k] = c.pin[k];
+    // limiterUpdate type 0 (limiter.c:49-59)
+    p.pref20[0] = c.pin[0] * c.pin[0];
+    p.pref20[1] = c.pin[1] * c.pin[1] + c.pin[2] * c.pin[2];
+    p.pref20[2] = p.pref20[1];
+    p.pref20[3] = c.pin[3] * c.pin[3];
+    for (int k = 4; k < x->nv; k++) p.pref20[k] = c.pin[k + 1] * c.pin[k + 1];
+    // solverCalcCoeff3 (solver.c:1348-1352)
+    p.p_inf = c.pin[3];
+    p.q_inf = 0.5 * c.pin[0] * (c.pin[1] * c.pin[1] + c.pin[2] * c.pin[2]);
+    p.sst_b1 = 0.075;
+    p.o_wall_factor = c.o_wall_factor;
+    p.tmax = 0;
+    p.conv_tol = 0;
+}
+
+static int reset_scalars(csu_ctx* x, int it0)
+{
+    Scalars h;
+    memset(&h, 0, sizeof(h));
+    h.dtmin_bits = 0x7ff0000000000000ULL;
+    h.dt_local = x->cfg.dt_local;
+    h.iter = it0;
+    CK(cudaMemcpyAsync(x->st.sc, &h, sizeof(h), cudaMemcpyHostToDevice, x->stream));
+    return CSU_OK;
+}
+
+static int read_scalars(csu_ctx* x, Scalars* h)
+{
+    CK(cudaMemcpyAsync(h, x->st.sc, sizeof(Scalars), cudaMemcpyDeviceToHost, x->stream));
+    CK(cudaStreamSynchronize(x->stream));
+    return CSU_OK;
+}
+
+extern "C" int csu_create(const csu_mesh_desc* md, const csu_config* cfg, csu_ctx** out)
+{
+    *out = nullptr;
+    if (!md || !cfg || md->n_cells <= 0) {
+        csu_set_error("csu_create: empty mesh or missing config");
+        return CSU_ERR_INPUT;
+    }
+    int model = cfg->sst ? 2 : (cfg->sa ? 1 : 0);
+    int nv = model == 0 ? 4 : (model == 1 ? 5 : 6);
+    if (cfg->nvar != nv) {
+        csu_set_error("csu_create: nvar %d does not match the turbulence model", cfg->nvar);
+        return CSU_ERR_INPUT;
+    }
+    if (model != 0 || cfg->laminar) {
+        csu_set_error("csu_create: viscous and turbulent models are not available in this engine build");
+        return CSU_ERR_UNSUPPORTED;
+    }
+    if (cfg->time_scheme == CSU_TS_LUSGS) {
+        csu_set_error("csu_create: LU-SGS is not available in this engine build");
+        return CSU_ERR_UNSUPPORTED;
+    }
+    if (cfg->time_scheme == CSU_TS_RK && !(cfg->stages == 1 || cfg->stages == 3 || cfg->stages == 4 ||
+                                            cfg->stages == 5)) {
+        csu_set_error("csu_create: RK with %d stages (the reference implements 1, 3, 4, 5)", cfg->stages);
+        return CSU_ERR_UNSUPPORTED;
+    }
+    if (cfg->time_scheme == CSU_TS_DPLUR && (cfg->n_linear < 1 || cfg->n_linear > MAX_SWEEPS)) {
+        csu_set_error("csu_create: Nlinear must be in [1, %d]", MAX_SWEEPS);
+        return CSU_ERR_UNSUPPORTED;
+    }
+    if (cfg->order != 1 && cfg->order != 2) {
+        csu_set_error("csu_create: order must be 1 or 2");
+        return CSU_ERR_INPUT;
+    }
+    if (cfg->limiter_type != 0) {
+        csu_set_error("csu_create: limiter type %d not available in this engine build", cfg->limiter_type);
+        return CSU_ERR_UNSUPPORTED;
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        csu_set_error("csu_create: no CUDA device");
+        return CSU_ERR_NO_DEVICE;
+    }
+    csu_ctx* x = new csu_ctx();
+    x->model = model;
+    x->nv = nv;
+    x->cfg = *cfg;
+    int st = csu_layout_build(md, cfg->axisymmetric, &x->L);
+    if (st) {
+        delete x;
+        csu_set_error("csu_create: mesh layout failed (a cell with more than four faces?)");
+        return st;
+    }
+    fill_params(x);
+    x->mesh.nc = x->L.nc;
+    x->mesh.nf = x->L.nf;
+    x->mesh.nb = x->L.nb;
+    // size, allocate once, carve
+    Arena a;
+    plan(x, a);
+    size_t bytes = a.size;
+    cudaError_t e = cudaMalloc((void**)&x->arena.base, bytes);
+    if (e != cudaSuccess) {
+        csu_layout_free(&x->L);
+        delete x;
+        return cuda_fail(e, "cudaMalloc(context arena)");
+    }
+    x->arena.size = bytes;
+    x->arena.used = 0;
+    plan(x, x->arena);
+    e = cudaMemset(x->arena.base, 0, bytes);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        cudaFree(x->arena.base);
+        csu_layout_free(&x->L);
+        delete x;
+        return cuda_fail(e, "context setup");
+    }
+    if ((st = upload_mesh(x)) || (st = reset_scalars(x, 0))) {
+        csu_destroy(x);
+        return st;
+    }
+    x->gb_c = (x->L.nc + BLOCK - 1) / BLOCK;
+    x->gb_fi = (x->L.nf + BLOCK - 1) / BLOCK;
+    x->gb_fb = (x->L.nb + BLOCK - 1) / BLOCK;
+    switch (cfg->stages) {
+    case 1: x->rk = RK1; break;
+    case 3: x->rk = RK3; break;
+    case 4: x->rk = RK4; break;
+    default: x->rk = RK5; break;
+    }
+    *out = x;
+    return CSU_OK;
+}
+
+extern "C" void csu_destroy(csu_ctx* x)
+{
+    if (!x) return;
+    if (x->graph) cudaGraphExecDestroy(x->graph);
+    if (x->st.hist) cudaFree(x->st.hist);
+    if (x->stream) cudaStreamDestroy(x->stream);
+    if (x->arena.base) cudaFree(x->arena.base);
+    csu_layout_free(&x->L);
+    delete x;
+}
+
+extern "C" int csu_set_state(csu_ctx* x, const double* U)
+{
+    const int nc = x->L.nc, nv = x->nv;
+    std::vector<double4> u4(nc);
+    std::vector<double> ux((size_t)(nv - 4) * nc + 1);
+    for (int c = 0; c < nc; c++) {
+        int o = x->L.cell_new2old[c];
+        u4[c] = make_double4(U[o], U[(size_t)nc + o], U[(size_t)2 * nc + o], U[(size_t)3 * nc + o]);
+        for (int k = 4; k < nv; k++) ux[(size_t)(k - 4) * nc + c] = U[(size_t)k * nc + o];
+    }
+    CK(cudaMemcpy(x->st.U4, u4.data(), sizeof(double4) * nc, cudaMemcpyHostToDevice));
+    if (nv > 4) CK(cudaMemcpy(x->st.Ux, ux.data(), sizeof(double) * (nv - 4) * nc, cudaMemcpyHostToDevice));
+    x->prepared = 0;
+    return CSU_OK;
+}
+
+extern "C" int csu_get_state(csu_ctx* x, double* U)
+{
+    const int nc = x->L.nc, nv = x->nv;
+    std::vector<double4> u4(nc);
+    std::vector<double> ux((size_t)(nv - 4) * nc + 1);
+    CK(cudaStreamSynchronize(x->stream));
+    CK(cudaMemcpy(u4.data(), x->st.U4, sizeof(double4) * nc, cudaMemcpyDeviceToHost));
+    if (nv > 4) CK(cudaMemcpy(ux.data(), x->st.Ux, sizeof(double) * (nv - 4) * nc, cudaMemcpyDeviceToHost));
+    for (int c = 0; c < nc; c++) {
+        int o = x->L.cell_new2old[c];
+        U[o] = u4[c].x;
+        U[(size_t)nc + o] = u4[c].y;
+        U[(size_t)2 * nc + o] = u4[c].z;
+        U[(size_t)3 * nc + o] = u4[c].w;
+        for (int k = 4; k < nv; k++) U[(size_t)k * nc + o] = ux[(size_t)(k - 4) * nc + c];
+    }
+    return CSU_OK;
+}
+
+extern "C" int csu_set_state_rows(csu_ctx* x, const double* const* U)
+{
+    const int nc = x->L.nc, nv = x->nv;
+    std::vector<double> flat((size_t)nv * nc);
+    for (int k = 0; k < nv; k++) memcpy(flat.data() + (size_t)k * nc, U[k], sizeof(double) * nc);
+    return csu_set_state(x, flat.data());
+}
+
+extern "C" int csu_get_state_rows(csu_ctx* x, double* const* U)
+{
+    const int nc = x->L.nc, nv = x->nv;
+    std::vector<double> flat((size_t)nv * nc);
+    int st = csu_get_state(x, flat.data());
+    if (st) return st;
+    for (int k = 0; k < nv; k++) memcpy(U[k], flat.data() + (size_t)k * nc, sizeof(double) * nc);
+    return CSU_OK;
+}
+
+// ---------------------------------------------------------------------------------------------- launches
+
+template <int MODEL>
+static void launch_grad(csu_ctx* x, bool dbg)
+{
+    if (dbg) k_grad<MODEL, true><<<x->gb_c, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st);
+    else k_grad<MODEL, false><<<x->gb_c, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st);
+    x->launches++;
+}
+
+template <int MODEL>
+static void launch_flux(csu_ctx* x, int coef)
+{
+    k_flux<MODEL><<<x->gb_fi + x->gb_fb, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st, x->gb_fi, x->d_wall_rank,
+                                                                 coef);
+    x->launches++;
+}
+
+template <int MODEL>
+static void launch_finalize(csu_ctx* x, int mode)
+{
+    k_finalize<MODEL><<<1, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st, x->gb_c, x->nwall, mode, x->hist_cap);
+    x->launches++;
+}
+
+template <int MODEL>
+static void launch_prologue(csu_ctx* x)
+{
+    int rk = x->cfg.time_scheme == CSU_TS_RK;
+    k_prim<MODEL><<<x->gb_c, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st, rk);
+    x->launches++;
+    launch_finalize<MODEL>(x, 2);
+}
+
+// one iteration of the steady loop body (solver.c:1866-1906)
+template <int MODEL>
+static void launch_iteration(csu_ctx* x)
+{
+    const csu_config& c = x->cfg;
+    if (c.time_scheme == CSU_TS_RK) {
+        for (int sgi = 0; sgi < c.stages; sgi++) {
+            bool last = sgi == c.stages - 1;
+            if (c.order == 2) launch_grad<MODEL>(x, false);
+            launch_flux<MODEL>(x, last ? 1 : 0);
+            if (last) k_rk<MODEL, true><<<x->gb_c, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st, x->rk[sgi]);
+            else k_rk<MODEL, false><<<x->gb_c, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st, x->rk[sgi]);
+            x->launches++;
+        }
+        launch_finalize<MODEL>(x, 0);
+    } else {
+        if (c.order == 2) launch_grad<MODEL>(x, false);
+        launch_flux<MODEL>(x, 1);
+        k_impl<MODEL, true><<<x->gb_c, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st);
+        x->launches++;
+        for (int m = 0; m < c.n_linear; m++) {
+            if (m == c.n_linear - 1)
+                k_sweep<MODEL, true><<<x->gb_c, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st, m, x->xcur);
+            else k_sweep<MODEL, false><<<x->gb_c, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st, m, x->xcur);
+            x->launches++;
+            x->xcur ^= 1;
+        }
+        launch_finalize<MODEL>(x, 1);
+    }
+}
+
+template <int MODEL>
+static void launch_residual(csu_ctx* x, bool dbg)
+{
+    k_prim<MODEL><<<x->gb_c, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st, 0);
+    x->launches++;
+    if (x->cfg.order == 2 || dbg) launch_grad<MODEL>(x, dbg);
+    launch_flux<MODEL>(x, 1);
+    k_resid<MODEL><<<x->gb_c, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st);
+    x->launches++;
+    launch_finalize<MODEL>(x, 3);
+}
+
+#define DISPATCH(fn, ...)                                                                                          \
+    do {                                                                                                           \
+        switch (x->model) {                                                                                        \
+        case 0: fn<0>(__VA_ARGS__); break;                                                                         \
+        case 1: fn<1>(__VA_ARGS__); break;                                                                         \
+        default: fn<2>(__VA_ARGS__); break;                                                                        \
+        }                                                                                                          \
+    } while (0)
+
+static int check_launch(const char* what)
+{
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, what);
+    return CSU_OK;
+}
+
+static int ensure_hist(csu_ctx* x, int n)
+{
+    if (n <= x->hist_cap) return CSU_OK;
+    int cap = n < 1024 ? 1024 : n;
+    if (x->st.hist) CK(cudaFree(x->st.hist));
+    x->st.hist = nullptr;
+    CK(cudaMalloc((void**)&x->st.hist, sizeof(double) * (size_t)cap * (x->nv + 4)));
+    x->hist_cap = cap;
+    if (x->graph) {
+        cudaGraphExecDestroy(x->graph);
+        x->graph = nullptr;
+    }
+    return CSU_OK;
+}
+
+// Captures `iters` iterations into a graph (the DPLUR buffer parity returns to its start value).
+static int build_graph(csu_ctx* x, int iters)
+{
+    if (x->graph) {
+        cudaGraphExecDestroy(x->graph);
+        x->graph = nullptr;
+    }
+    int xcur0 = x->xcur;
+    long long l0 = x->launches;
+    cudaGraph_t g;
+    CK(cudaStreamBeginCapture(x->stream, cudaStreamCaptureModeThreadLocal));
+    for (int i = 0; i < iters; i++) DISPATCH(launch_iteration, x);
+    cudaError_t e = cudaStreamEndCapture(x->stream, &g);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+    e = cudaGraphInstantiate(&x->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
+    x->graph_iters = iters;
+    x->xcur = xcur0;
+    x->launches = l0;
+    return CSU_OK;
+}
+
+static int run_iterations(csu_ctx* x, int n, int it0, Scalars* out)
+{
+    int st;
+    if ((st = ensure_hist(x, n))) return st;
+    if (!x->prepared) {
+        if ((st = reset_scalars(x, it0))) return st;
+        DISPATCH(launch_prologue, x);
+        if ((st = check_launch("prologue"))) return st;
+        x->prepared = 1;
+    } else {
+        // keep the device step state, restart the history rows and the loop counter
+        Scalars h;
+        if ((st = read_scalars(x, &h))) return st;
+        h.hist_row = 0;
+        h.iter = it0;
+        h.steps = 0;
+        CK(cudaMemcpyAsync(x->st.sc, &h, sizeof(h), cudaMemcpyHostToDevice, x->stream));
+    }
+    // graphs of G iterations; G even so the DPLUR increment buffers come back to the same parity
+    const int G = 8;
+    int done = 0;
+    if (n >= G) {
+        if (!x->graph || x->graph_iters != G)
+            if ((st = build_graph(x, G))) return st;
+        while (n - done >= G) {
+            CK(cudaGraphLaunch(x->graph, x->stream));
+            int per = x->cfg.time_scheme == CSU_TS_RK ? x->cfg.stages * (x->cfg.order == 2 ? 3 : 2) + 1
+                                                       : (x->cfg.order == 2 ? 3 : 2) + x->cfg.n_linear + 1;
+            x->launches += (long long)per * G;
+            done += G;
+        }
+    }
+    for (; done < n; done++) DISPATCH(launch_iteration, x);
+    if ((st = check_launch("iteration"))) return st;
+    if ((st = read_scalars(x, out))) return st;
+    return CSU_OK;
+}
+
+extern "C" int csu_iterate(csu_ctx* x, int n, int it0, double* hist)
+{
+    if (!x || n < 0) return CSU_ERR_INPUT;
+    if (n == 0) return CSU_OK;
+    Scalars h;
+    int st = run_iterations(x, n, it0, &h);
+    if (st) return st;
+    if (hist) {
+        int rows = h.hist_row < n ? h.hist_row : n;
+        CK(cudaMemcpy(hist, x->st.hist, sizeof(double) * (size_t)rows * (x->nv + 4), cudaMemcpyDeviceToHost));
+    }
+    if (h.status) {
+        csu_set_error("csu_iterate: state became non-finite at iteration %d", h.iter);
+        return h.status;
+    }
+    return CSU_OK;
+}
+
+extern "C" int csu_tube_run(csu_ctx* x, double tmax, int* steps, double* t_final)
+{
+    if (!x->cfg.tube || x->cfg.time_scheme != CSU_TS_RK) {
+        csu_set_error("csu_tube_run: the case is not a tube case with RK time stepping");
+        return CSU_ERR_STATE;
+    }
+    x->prm.tube = 1;
+    x->prm.tmax = tmax;
+    x->prepared = 0;
+    if (x->graph) {
+        cudaGraphExecDestroy(x->graph);
+        x->graph = nullptr;
+    }
+    Scalars h;
+    int st, total = 0;
+    memset(&h, 0, sizeof(h));
+    // the loop of solver.c:1921-1940 runs until the step that reaches tmax; checked every 64 steps
+    for (int guard = 0; guard < 20000; guard++) {
+        if ((st = run_iterations(x, 64, total, &h))) return st;
+        total = h.iter;
+        if (h.done || h.status) break;
+    }
+    if (x->graph) {
+        cudaGraphExecDestroy(x->graph);
+        x->graph = nullptr;
+    }
+    *steps = total;
+    *t_final = h.t;
+    if (h.status) {
+        csu_set_error("csu_tube_run: state became non-finite at step %d", total);
+        return h.status;
+    }
+    return CSU_OK;
+}
+
+extern "C" int csu_residual(csu_ctx* x, double* R)
+{
+    if (!x) return CSU_ERR_INPUT;
+    int st;
+    // a fresh evaluation: scalars keep the step state but not a halt flag
+    Scalars h;
+    if ((st = read_scalars(x, &h))) return st;
+    h.done = 0;
+    h.status = 0;
+    CK(cudaMemcpyAsync(x->st.sc, &h, sizeof(h), cudaMemcpyHostToDevice, x->stream));
+    DISPATCH(launch_residual, x, true);
+    if ((st = check_launch("residual"))) return st;
+    x->prepared = 0;
+    CK(cudaStreamSynchronize(x->stream));
+    if (R) return csu_dump(x, CSU_DUMP_R, R);
+    return CSU_OK;
+}
+
+extern "C" int csu_dump(csu_ctx* x, int what, double* out)
+{
+    const int nc = x->L.nc, nf = x->L.nf, nb = x->L.nb, nv = x->nv, nx = nv - 4;
+    CK(cudaStreamSynchronize(x->stream));
+    auto d2h = [&](std::vector<double>& v, const void* src, size_t n) -> cudaError_t {
+        v.resize(n > 0 ? n : 1);
+        if (n == 0) return cudaSuccess;
+        return cudaMemcpy(v.data(), src, sizeof(double) * n, cudaMemcpyDeviceToHost);
+    };
+    std::vector<double> a, b, c2;
+    const int* n2o = x->L.cell_new2old;
+    switch (what) {
+    case CSU_DUMP_P: {
+        CK(d2h(a, x->st.W4, (size_t)4 * nc));
+        CK(d2h(b, x->st.WT, nc));
+        CK(d2h(c2, x->st.Wx, (size_t)nx * nc));
+        for (int c = 0; c < nc; c++) {
+            double* row = out + (size_t)n2o[c] * (nv + 1);
+            for (int k = 0; k < 4; k++) row[k] = a[(size_t)4 * c + k];
+            row[4] = b[c];
+            for (int k = 5; k < nv + 1; k++) row[k] = c2[(size_t)(k - 5) * nc + c];
+        }
+        return CSU_OK;
+    }
+    case CSU_DUMP_GHOST_P:
+        CK(d2h(a, x->st.dbg_ghost, (size_t)nb * (nv + 1)));
+        memcpy(out, a.data(), sizeof(double) * (size_t)nb * (nv + 1));
+        return CSU_OK;
+    case CSU_DUMP_GRAD:
+    case CSU_DUMP_PHI: {
+        const double4* s4[2] = {x->st.G4x, x->st.G4y};
+        const double* sx[2] = {x->st.Gxx, x->st.Gxy};
+        int nparts = what == CSU_DUMP_GRAD ? 2 : 1;
+        if (what == CSU_DUMP_PHI) {
+            s4[0] = x->st.PH4;
+            sx[0] = x->st.PHx;
+        }
+        for (int part = 0; part < nparts; part++) {
+            CK(d2h(a, s4[part], (size_t)4 * nc));
+            CK(d2h(b, sx[part], (size_t)nx * nc));
+            double* o = out + (size_t)part * nv * nc;
+            for (int c = 0; c < nc; c++) {
+                for (int k = 0; k < 4; k++) o[(size_t)k * nc + n2o[c]] = a[(size_t)4 * c + k];
+                for (int k = 4; k < nv; k++) o[(size_t)k * nc + n2o[c]] = b[(size_t)(k - 4) * nc + c];
+            }
+        }
+        return CSU_OK;
+    }
+    case CSU_DUMP_FACEFLUX: {
+        CK(d2h(a, x->st.F4, (size_t)4 * (nf + nb)));
+        CK(d2h(b, x->st.Fx, (size_t)nx * (nf + nb)));
+        for (int f = 0; f < nf; f++) {
+            int o = x->L.face_new2old[f];
+            for (int k = 0; k < 4; k++) out[(size_t)k * nf + o] = a[(size_t)4 * f + k];
+            for (int k = 4; k < nv; k++) out[(size_t)k * nf + o] = b[(size_t)(k - 4) * (nf + nb) + f];
+        }
+        return CSU_OK;
+    }
+    case CSU_DUMP_R:
+    case CSU_DUMP_DW: {
+        const double4* s4 = what == CSU_DUMP_R ? x->st.R4 : x->st.X4[x->xcur];
+        const double* sx = what == CSU_DUMP_R ? x->st.Rx : x->st.Xx[x->xcur];
+        if (!s4) {
+            csu_set_error("csu_dump: no implicit increment in this context");
+            return CSU_ERR_STATE;
+        }
+        CK(d2h(a, s4, (size_t)4 * nc));
+        CK(d2h(b, sx, (size_t)nx * nc));
+        for (int c = 0; c < nc; c++) {
+            for (int k = 0; k < 4; k++) out[(size_t)k * nc + n2o[c]] = a[(size_t)4 * c + k];
+            for (int k = 4; k < nv; k++) out[(size_t)k * nc + n2o[c]] = b[(size_t)(k - 4) * nc + c];
+        }
+        return CSU_OK;
+    }
+    case CSU_DUMP_D:
+    case CSU_DUMP_DTL: {
+        CK(d2h(a, what == CSU_DUMP_D ? x->st.dpart : x->st.dtl, nc));
+        if (what == CSU_DUMP_D) {
+            // D = dpart + Omega/dt with the step of the last implicit iteration (implicit.c:167-180)
+            Scalars h;
+            int st = read_scalars(x, &h);
+            if (st) return st;
+            (void)h;
+            std::vector<double> dtl;
+            CK(d2h(dtl, x->st.dtl, nc));
+            double mn = dtl[0];
+            for (int c = 1; c < nc; c++) mn = fmin(mn, dtl[c]);
+            double dt = mn * x->cfg.cfl;
+            for (int c = 0; c < nc; c++) out[n2o[c]] = a[c] + x->L.omega[c] / dt;
+        } else {
+            for (int c = 0; c < nc; c++) out[n2o[c]] = a[c];
+        }
+        return CSU_OK;
+    }
+    case CSU_DUMP_BLOCKS: {
+        if (!x->st.blocks) {
+            csu_set_error("csu_dump: no DPLUR blocks in this context");
+            return CSU_ERR_STATE;
+        }
+        size_t per = (size_t)nv * nv;
+        CK(d2h(a, x->st.blocks, (size_t)4 * per * nc));
+        for (int c = 0; c < nc; c++) {
+            double* o = out + (size_t)n2o[c] * 4 * per;
+            for (int j = 0; j < 4; j++)
+                for (size_t e = 0; e < per; e++) o[j * per + e] = a[((size_t)j * per + e) * nc + c];
+        }
+        return CSU_OK;
+    }
+    default:
+        csu_set_error("csu_dump: unknown view %d", what);
+        return CSU_ERR_INPUT;
+    }
+}
+
+extern "C" int csu_stats(csu_ctx* x, long long* launches, long long* bytes)
+{
+    if (launches) *launches = x->launches;
+    if (bytes) *bytes = (long long)x->arena.size + (long long)x->hist_cap * (x->nv + 4) * 8;
+    return CSU_OK;
+}

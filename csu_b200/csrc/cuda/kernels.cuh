@@ -1,0 +1,647 @@
+// kernels.cuh -- the residual-and-update kernels.
+//
+// One residual evaluation (solverCalcR, solver.c:685) is three passes over HBM:
+//   k_grad   per cell:  gathers neighbour primitives (ghost states of boundary neighbours are evaluated on
+//                       the fly from the cell's own state: a ghost is only ever its owner's neighbour),
+//                       least-squares gradient + Venkatakrishnan limiter          (solver.c:451-548)
+//   k_flux   per face:  MUSCL states, rotation, Riemann flux * |dS| for interior faces, first-order
+//                       boundary fluxes for boundary faces; one launch, block-uniform split (inter 550-644,
+//                       boundary.c:143-443)
+//   k_rk / k_impl per cell: gathers the signed face fluxes in the reference's order (inter 646-667, then
+//                       boundary faces, then the axisymmetric source) and fuses the state update that follows
+//                       (solverRK, or the implicit diagonal and DPLUR blocks), the next stage's primitives
+//                       with their clamps, local time steps and residual-norm partial sums.
+// Nothing is scattered, so no atomics are needed on the state; the only atomics are order-free min/max of
+// scalars. Kernels exit immediately once the solve's device status says "done" or "error", so whole
+// iteration sequences can be captured in one CUDA graph.
+#pragma once
+#include "engine.cuh"
+
+namespace csu {
+
+__device__ __forceinline__ bool halted(const State& s)
+{
+    return (s.sc->status | s.sc->done) != 0;
+}
+
+// ------------------------------------------------------------------------------------------------
+// k_prim: W = primitives of clamp(U), U := clamp(U) (solverCalcPrimitive cell loop). With dt: the local
+// step of the unclamped state first (solverCalcDt precedes solverCalcR, solver.c:1868-1869).
+// ------------------------------------------------------------------------------------------------
+template <int MODEL>
+__global__ void __launch_bounds__(BLOCK) k_prim(const __grid_constant__ Prm p, const __grid_constant__ Mesh m,
+                                                const __grid_constant__ State s, int with_dt)
+{
+    constexpr int NV = Model<MODEL>::NV, NP = Model<MODEL>::NP;
+    int c = blockIdx.x * BLOCK + threadIdx.x;
+    double lmin = __longlong_as_double(0x7ff0000000000000LL);
+    if (c < m.nc) {
+        double U[NV], P[NP];
+        loadU<MODEL>(s, m.nc, c, U);
+        if (with_dt) {
+            double l = local_step<MODEL>(p, U, m.sxh[c], m.syh[c], m.omega[c]);
+            s.dtl[c] = p.cfl * l;
+            lmin = l;
+        }
+        clamp_prim<MODEL>(p, U, P);
+        storeU<MODEL>(s, m.nc, c, U);
+        storeP<MODEL>(s, m.nc, c, P);
+    }
+    if (with_dt) {
+        double v = warp_min(lmin);
+        if ((threadIdx.x & 31) == 0 && !(v > bitsd(0x7fefffffffffffffULL))) atomicMin(&s.sc->dtmin_bits, dbits(v));
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// k_grad: solverUpdateGrad + the limiter loop of inter (solver.c:451-548).
+// DBG also records ghost primitives (boundaryCalcPrimitive) in reference order.
+// ------------------------------------------------------------------------------------------------
+template <int MODEL, bool DBG>
+__global__ void __launch_bounds__(BLOCK) k_grad(const __grid_constant__ Prm p, const __grid_constant__ Mesh m,
+                                                const __grid_constant__ State s)
+{
+    constexpr int NV = Model<MODEL>::NV, NP = Model<MODEL>::NP;
+    int c = blockIdx.x * BLOCK + threadIdx.x;
+    if (c >= m.nc || halted(s)) return;
+    const int nc = m.nc;
+    double P0[NP];
+    loadP<MODEL>(s, nc, c, P0);
+    double gx[NV], gy[NV], qmin[NV], qmax[NV];
+#pragma unroll
+    for (int kk = 0; kk < NV; kk++) {
+        gx[kk] = 0.0;
+        gy[kk] = 0.0;
+        qmin[kk] = P0[slot2p(kk)];
+        qmax[kk] = P0[slot2p(kk)];
+    }
+    const int np = m.npts[c];
+    const double dw = m.wall_d ? m.wall_d[c] : 0.0;
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        if (j < np) {
+            int n = m.nei[(size_t)j * nc + c];
+            double Pn[NP];
+            if (n < nc) {
+                loadP<MODEL>(s, nc, n, Pn);
+            } else {
+                int b = n - nc;
+                double2 dSv = m.bn[b];
+                ghost_state<MODEL>(p, m.bflag[b], dSv.x, dSv.y, m.bds[b], P0, dw, Pn);
+                if (DBG) {
+                    int bo = m.bold[b];
+                    for (int k = 0; k < NP; k++) s.dbg_ghost[(size_t)bo * NP + k] = Pn[k];
+                }
+            }
+            double wxj = m.wx[(size_t)j * nc + c], wyj = m.wy[(size_t)j * nc + c];
+#pragma unroll
+            for (int kk = 0; kk < NV; kk++) {
+                double du = Pn[slot2p(kk)] - P0[slot2p(kk)];
+                gx[kk] += wxj * du;
+                gy[kk] += wyj * du;
+                qmax[kk] = fmax(qmax[kk], Pn[slot2p(kk)]);
+                qmin[kk] = fmin(qmin[kk], Pn[slot2p(kk)]);
+            }
+        }
+    }
+    double phi[NV];
+#pragma unroll
+    for (int kk = 0; kk < NV; kk++) phi[kk] = 1.0;
+    if (p.order == 2) {
+        // limiterCalc (limiter.c:98-119), type 0: eps^2 = q_inf^2 (K sqrt(omega/omega_max))^3
+        double aux = p.lim_k * sqrt(m.omega[c] / p.vol_max);
+        aux = aux * aux * aux;
+        double ee[NV];
+#pragma unroll
+        for (int kk = 0; kk < NV; kk++) {
+            if (p.limiter_type == 0) {
+                ee[kk] = p.pref20[kk] * aux;
+            } else {
+                int mm = kk == 4 ? 5 : kk; // limiter.c:66-70 (SST reads k for both scalars)
+                int sl = mm > 4 ? mm - 1 : mm;
+                double a2 = (ordbits_inv(s.sc->qmax_bits[sl]) - ordbits_inv(s.sc->qmin_bits[sl])) * p.lim_k;
+                ee[kk] = a2 * a2;
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            if (j < np) {
+                double exj = m.ex[(size_t)j * nc + c], eyj = m.ey[(size_t)j * nc + c];
+#pragma unroll
+                for (int kk = 0; kk < NV; kk++) {
+                    double d2 = (gx[kk] * exj + gy[kk] * eyj);
+                    double phi0 = limiterV2(P0[slot2p(kk)], qmin[kk], qmax[kk], d2, ee[kk]);
+                    phi[kk] = j == 0 ? phi0 : fmin(phi[kk], phi0);
+                }
+            }
+        }
+    }
+    s.G4x[c] = make_double4(gx[0], gx[1], gx[2], gx[3]);
+    s.G4y[c] = make_double4(gy[0], gy[1], gy[2], gy[3]);
+    s.PH4[c] = make_double4(phi[0], phi[1], phi[2], phi[3]);
+#pragma unroll
+    for (int kk = 4; kk < NV; kk++) {
+        s.Gxx[(size_t)(kk - 4) * nc + c] = gx[kk];
+        s.Gxy[(size_t)(kk - 4) * nc + c] = gy[kk];
+        s.PHx[(size_t)(kk - 4) * nc + c] = phi[kk];
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// k_flux: interior faces (blocks [0, nbi)) and boundary faces (blocks [nbi, ...)).
+// coef: also record the wall pressure-coefficient terms of solverCalcCoeff3 (solver.c:1360-1385).
+// ------------------------------------------------------------------------------------------------
+template <int MODEL>
+__global__ void __launch_bounds__(BLOCK) k_flux(const __grid_constant__ Prm p, const __grid_constant__ Mesh m,
+                                                const __grid_constant__ State s, int nbi, const int* wall_rank,
+                                                int coef)
+{
+    constexpr int NV = Model<MODEL>::NV, NP = Model<MODEL>::NP;
+    if (halted(s)) return;
+    const int nc = m.nc;
+    if ((int)blockIdx.x < nbi) {
+        int f = blockIdx.x * BLOCK + threadIdx.x;
+        if (f >= m.nf) return;
+        int2 e = m.fe[f];
+        double2 dSv = m.fn[f];
+        double dSx = dSv.x, dSy = dSv.y, dS = m.fds[f];
+        double PL[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        double PR[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        double A[NP], B[NP];
+        loadP<MODEL>(s, nc, e.x, A);
+        loadP<MODEL>(s, nc, e.y, B);
+        if (p.order == 2) {
+            double2 r0 = m.r0[f], r1 = m.r1[f];
+            double4 gx0 = s.G4x[e.x], gy0 = s.G4y[e.x], ph0 = s.PH4[e.x];
+            double4 gx1 = s.G4x[e.y], gy1 = s.G4y[e.y], ph1 = s.PH4[e.y];
+            double g0x[4] = {gx0.x, gx0.y, gx0.z, gx0.w}, g0y[4] = {gy0.x, gy0.y, gy0.z, gy0.w};
+            double g1x[4] = {gx1.x, gx1.y, gx1.z, gx1.w}, g1y[4] = {gy1.x, gy1.y, gy1.z, gy1.w};
+            double f0[4] = {ph0.x, ph0.y, ph0.z, ph0.w}, f1[4] = {ph1.x, ph1.y, ph1.z, ph1.w};
+#pragma unroll
+            for (int kk = 0; kk < 4; kk++) {
+                PL[kk] = A[kk] + (g0x[kk] * r0.x + g0y[kk] * r0.y) * f0[kk];
+                PR[kk] = B[kk] + (g1x[kk] * r1.x + g1y[kk] * r1.y) * f1[kk];
+            }
+#pragma unroll
+            for (int kk = 4; kk < NV; kk++) {
+                if (p.turb1order) {
+                    PL[kk] = A[kk + 1];
+                    PR[kk] = B[kk + 1];
+                } else {
+                    size_t o = (size_t)(kk - 4) * nc;
+                    PL[kk] = A[kk + 1] + (s.Gxx[o + e.x] * r0.x + s.Gxy[o + e.x] * r0.y) * s.PHx[o + e.x];
+                    PR[kk] = B[kk + 1] + (s.Gxx[o + e.y] * r1.x + s.Gxy[o + e.y] * r1.y) * s.PHx[o + e.y];
+                }
+            }
+        } else {
+#pragma unroll
+            for (int kk = 0; kk < NV; kk++) {
+                PL[kk] = A[slot2p(kk)];
+                PR[kk] = B[slot2p(kk)];
+            }
+        }
+        rotation(PL, dSx, dSy, dS);
+        rotation(PR, dSx, dSy, dS);
+        double fl[NV];
+        riemann<MODEL>(p.scheme, p.gas, p.e_fix, p.mach_inf, PL, PR, fl);
+        rotation(fl, dSx, -dSy, dS);
+        s.F4[f] = make_double4(fl[0] * dS, fl[1] * dS, fl[2] * dS, fl[3] * dS);
+#pragma unroll
+        for (int kk = 4; kk < NV; kk++) s.Fx[(size_t)(kk - 4) * (m.nf + m.nb) + f] = fl[kk] * dS;
+    } else {
+        int b = (blockIdx.x - nbi) * BLOCK + threadIdx.x;
+        if (b >= m.nb) return;
+        int c = m.bown[b];
+        int flag = m.bflag[b];
+        double2 dSv = m.bn[b];
+        double dSx = dSv.x, dSy = dSv.y, dS = m.bds[b];
+        double E0[NP];
+        loadP<MODEL>(s, nc, c, E0);
+        double fl[NV];
+        boundary_flux<MODEL>(p, flag, dSx, dSy, dS, E0, fl);
+        int fi = m.nf + b;
+        double sc = dS > 0 ? dS : 0.0;
+        s.F4[fi] = dS > 0 ? make_double4(fl[0] * dS, fl[1] * dS, fl[2] * dS, fl[3] * dS)
+                          : make_double4(0.0, 0.0, 0.0, 0.0);
+#pragma unroll
+        for (int kk = 4; kk < NV; kk++) s.Fx[(size_t)(kk - 4) * (m.nf + m.nb) + fi] = dS > 0 ? fl[kk] * sc : 0.0;
+        if (coef && (flag == 3 || flag == 4)) {
+            double G[NP];
+            ghost_state<MODEL>(p, flag, dSx, dSy, dS, E0, m.wall_d ? m.wall_d[c] : 0.0, G);
+            double cp = (G[3] - p.p_inf) / p.q_inf;
+            int r = wall_rank[b];
+            s.bcoef[(size_t)r * 4 + 0] = cp * dSx;
+            s.bcoef[(size_t)r * 4 + 1] = cp * dSy;
+            s.bcoef[(size_t)r * 4 + 2] = 0.0;
+            s.bcoef[(size_t)r * 4 + 3] = 0.0;
+        }
+    }
+}
+
+// Sum of the signed face fluxes of one cell in the reference's order (inter, then boundary, then the
+// axisymmetric pressure source interAxisPressure, solver.c:646-683).
+template <int MODEL>
+__device__ __forceinline__ void gather_residual(const Prm& p, const Mesh& m, const State& s, int c, const double* P,
+                                                double* R)
+{
+    constexpr int NV = Model<MODEL>::NV;
+    const int nc = m.nc, nft = m.nf + m.nb;
+#pragma unroll
+    for (int k = 0; k < NV; k++) R[k] = 0.0;
+    const int ns = m.nslot[c];
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        if (j < ns) {
+            int sf = m.fslot[(size_t)j * nc + c];
+            int fi = sf > 0 ? sf - 1 : -sf - 1;
+            double4 F = s.F4[fi];
+            double fv[NV];
+            fv[0] = F.x; fv[1] = F.y; fv[2] = F.z; fv[3] = F.w;
+#pragma unroll
+            for (int k = 4; k < NV; k++) fv[k] = s.Fx[(size_t)(k - 4) * nft + fi];
+            if (sf > 0) {
+#pragma unroll
+                for (int k = 0; k < NV; k++) R[k] += fv[k];
+            } else {
+#pragma unroll
+                for (int k = 0; k < NV; k++) R[k] -= fv[k];
+            }
+        }
+    }
+    if (p.axi == 1) {
+        double dS = m.dslat[c];
+        R[2] -= P[3] * dS;
+        if constexpr (MODEL == 2) R[2] -= (2. / 3.) * P[0] * P[5] * dS;
+    }
+}
+
+template <int MODEL>
+__device__ __forceinline__ void storeR(const State& s, int nc, int c, const double* R)
+{
+    s.R4[c] = make_double4(R[0], R[1], R[2], R[3]);
+#pragma unroll
+    for (int k = 4; k < Model<MODEL>::NV; k++) s.Rx[(size_t)(k - 4) * nc + c] = R[k];
+}
+
+template <int MODEL>
+__device__ __forceinline__ void partial_norms(const State& s, bool valid, const double* R)
+{
+    constexpr int NV = Model<MODEL>::NV;
+    __shared__ double sh[NV][BLOCK / 32];
+    double v[NV];
+#pragma unroll
+    for (int k = 0; k < NV; k++) v[k] = valid ? R[k] * R[k] : 0.0;
+    block_sum<NV>(v, sh);
+    if (threadIdx.x == 0)
+        for (int k = 0; k < NV; k++) s.part[(size_t)blockIdx.x * NV + k] = v[k];
+}
+
+// ------------------------------------------------------------------------------------------------
+// k_resid: R only (csu_residual).
+// ------------------------------------------------------------------------------------------------
+template <int MODEL>
+__global__ void __launch_bounds__(BLOCK) k_resid(const __grid_constant__ Prm p, const __grid_constant__ Mesh m,
+                                                 const __grid_constant__ State s)
+{
+    constexpr int NV = Model<MODEL>::NV, NP = Model<MODEL>::NP;
+    int c = blockIdx.x * BLOCK + threadIdx.x;
+    bool valid = c < m.nc;
+    double R[NV];
+    if (valid) {
+        double P[NP];
+        loadP<MODEL>(s, m.nc, c, P);
+        gather_residual<MODEL>(p, m, s, c, P, R);
+        storeR<MODEL>(s, m.nc, c, R);
+    }
+    partial_norms<MODEL>(s, valid, R);
+}
+
+// ------------------------------------------------------------------------------------------------
+// k_rk: one RK stage update (solverRK, solver.c:741-766) fused with the next residual's primitives.
+// LAST: the stage that ends the iteration -- stores the state, the next local steps (solverCalcDt on the
+// new, unclamped state) and the residual-norm partial sums of this stage's R (solverCalcRes).
+// ------------------------------------------------------------------------------------------------
+template <int MODEL, bool LAST>
+__global__ void __launch_bounds__(BLOCK) k_rk(const __grid_constant__ Prm p, const __grid_constant__ Mesh m,
+                                              const __grid_constant__ State s, double a)
+{
+    constexpr int NV = Model<MODEL>::NV, NP = Model<MODEL>::NP;
+    if (halted(s)) return;
+    int c = blockIdx.x * BLOCK + threadIdx.x;
+    bool valid = c < m.nc;
+    double R[NV];
+    double lmin = bitsd(0x7ff0000000000000ULL);
+    if (valid) {
+        double P[NP], U[NV];
+        loadP<MODEL>(s, m.nc, c, P);
+        gather_residual<MODEL>(p, m, s, c, P, R);
+        loadU<MODEL>(s, m.nc, c, U);
+        double om = m.omega[c];
+        double dt = s.sc->dt_local == 1 ? s.dtl[c] : s.sc->dt;
+#pragma unroll
+        for (int k = 0; k < NV; k++) U[k] = U[k] - dt * p.sigma * a * R[k] / om;
+        if (LAST) {
+            double l = local_step<MODEL>(p, U, m.sxh[c], m.syh[c], om);
+            s.dtl[c] = p.cfl * l;
+            lmin = l;
+            clamp_prim<MODEL>(p, U, P);
+            storeU<MODEL>(s, m.nc, c, U);
+            storeR<MODEL>(s, m.nc, c, R);
+        } else {
+            clamp_prim<MODEL>(p, U, P);
+        }
+        storeP<MODEL>(s, m.nc, c, P);
+    }
+    if (LAST) {
+        double v = warp_min(lmin);
+        if ((threadIdx.x & 31) == 0 && !(v > bitsd(0x7fefffffffffffffULL))) atomicMin(&s.sc->dtmin_bits, dbits(v));
+        partial_norms<MODEL>(s, valid, R);
+    }
+}
+
+// implicitAuxCalcFlux2 (implicit.c:183-191) and its _sa/_sst forms
+template <int NV>
+__device__ __forceinline__ void aux_flux(const double* U, double pr, double nx, double ny, double* F)
+{
+    double V = (nx * U[1] + ny * U[2]) / U[0];
+    F[0] = U[0] * V;
+    F[1] = U[1] * V + nx * pr;
+    F[2] = U[2] * V + ny * pr;
+    F[3] = (U[3] + pr) * V;
+#pragma unroll
+    for (int k = 4; k < NV; k++) F[k] = U[k] * V;
+}
+
+// ------------------------------------------------------------------------------------------------
+// k_impl: R, the implicit diagonal (implicitCalcD, implicit.c:19-181) and, with BLOCKS, the DPLUR
+// off-diagonal blocks of implicitUpdateA (implicit.c:689-813) for each interior face of the cell.
+// ------------------------------------------------------------------------------------------------
+template <int MODEL, bool BLOCKS>
+__global__ void __launch_bounds__(BLOCK) k_impl(const __grid_constant__ Prm p, const __grid_constant__ Mesh m,
+                                                const __grid_constant__ State s)
+{
+    constexpr int NV = Model<MODEL>::NV, NP = Model<MODEL>::NP;
+    if (halted(s)) return;
+    int c = blockIdx.x * BLOCK + threadIdx.x;
+    bool valid = c < m.nc;
+    double R[NV];
+    double lmin = bitsd(0x7ff0000000000000ULL);
+    if (valid) {
+        const int nc = m.nc;
+        double P[NP];
+        loadP<MODEL>(s, nc, c, P);
+        gather_residual<MODEL>(p, m, s, c, P, R);
+        storeR<MODEL>(s, nc, c, R);
+        const int ni = m.nint[c], ns = m.nslot[c];
+        double Lc = 0;
+        for (int j = 0; j < ni; j++) {
+            int sf = m.fslot[(size_t)j * nc + c];
+            int f = sf > 0 ? sf - 1 : -sf - 1;
+            int2 e = m.fe[f];
+            double4 w0 = s.W4[e.x], w1 = s.W4[e.y];
+            double T0 = s.WT[e.x], T1 = s.WT[e.y];
+            double2 dSv = m.fn[f];
+            double dS = m.fds[f];
+            double u = (w0.y + w1.y) * 0.5;
+            double v = (w0.z + w1.z) * 0.5;
+            double T = (T0 + T1) * 0.5;
+            double cc = T2c(p.gas, T);
+            double nx = dSv.x / dS, ny = dSv.y / dS;
+            Lc += (fabs(nx * u + ny * v) + cc) * dS;
+        }
+        double D = 0.5 * p.w_imp * Lc;
+        for (int j = ni; j < ns; j++) {
+            int b = m.fslot[(size_t)j * nc + c] - 1 - m.nf;
+            double2 dSv = m.bn[b];
+            double dS = m.bds[b];
+            double cc = T2c(p.gas, P[4]);
+            double nx, ny;
+            if (dS > 0) {
+                nx = dSv.x / dS;
+                ny = dSv.y / dS;
+            } else {
+                nx = 0.0;
+                ny = 1.0;
+            }
+            double Lb = (fabs(nx * P[1] + ny * P[2]) + cc) * dS;
+            Lc += Lb;
+            D += 0.5 * p.w_imp * Lb;
+        }
+        double om = m.omega[c];
+        double l = om / Lc;
+        s.dtl[c] = l;
+        s.dpart[c] = D;
+        lmin = l;
+        if (BLOCKS) {
+            const double h = 1.0e-6;
+            for (int j = 0; j < ni; j++) {
+                int sf = m.fslot[(size_t)j * nc + c];
+                int f = sf > 0 ? sf - 1 : -sf - 1;
+                int2 e = m.fe[f];
+                int nb = sf > 0 ? e.y : e.x;
+                double2 dSv = m.fn[f];
+                double dSx = sf > 0 ? dSv.x : -dSv.x, dSy = sf > 0 ? dSv.y : -dSv.y;
+                double dS = m.fds[f];
+                double nx = dSx / dS, ny = dSy / dS;
+                double Un[NV], Pn[NP];
+                loadU<MODEL>(s, nc, nb, Un);
+                loadP<MODEL>(s, nc, nb, Pn);
+                double F0[NV], F[NV], Uq[NV];
+                double rho = Un[0];
+                double uu = Un[1] / rho;
+                double vv = Un[2] / rho;
+                double E = Un[3] / rho;
+                aux_flux<NV>(Un, Pn[3], nx, ny, F0);
+                double ee0 = E - 0.5 * (uu * uu + vv * vv);
+                double* A = s.blocks + (size_t)j * NV * NV * nc + c;
+#pragma unroll
+                for (int mm = 0; mm < NV; mm++) {
+#pragma unroll
+                    for (int nn = 0; nn < NV; nn++) Uq[nn] = mm == nn ? Un[nn] + h : Un[nn];
+                    double r2 = Uq[0];
+                    double u2 = Uq[1] / r2;
+                    double v2 = Uq[2] / r2;
+                    double E2 = Uq[3] / r2;
+                    double ee1 = E2 - 0.5 * (u2 * u2 + v2 * v2);
+                    double T = e2Taprox(p.gas, ee0, Pn[4], ee1);
+                    double pr = p.gas.R * r2 * T;
+                    aux_flux<NV>(Uq, pr, nx, ny, F);
+#pragma unroll
+                    for (int nn = 0; nn < NV; nn++) A[(size_t)(nn * NV + mm) * nc] = 0.5 * (F[nn] - F0[nn]) * dS / h;
+                }
+                double cc = T2c(p.gas, Pn[4]);
+                double ra = p.w_imp * (fabs(nx * Pn[1] + ny * Pn[2]) + cc) * dS;
+#pragma unroll
+                for (int nn = 0; nn < NV; nn++) A[(size_t)(nn * NV + nn) * nc] -= 0.5 * ra;
+            }
+        }
+    }
+    double v = warp_min(lmin);
+    if ((threadIdx.x & 31) == 0 && !(v > bitsd(0x7fefffffffffffffULL))) atomicMin(&s.sc->dtmin_bits, dbits(v));
+    partial_norms<MODEL>(s, valid, R);
+}
+
+// ------------------------------------------------------------------------------------------------
+// k_sweep: one relaxed Jacobi sweep of implicitCalcDPLUR (implicit.c:1006-1033, implicitMultA 938-972):
+//   x_new = w (-R - (D x + sum_j A_j x_j)) / D + x,  w = 2/3,  D += Omega/dt with dt = CFL min(Omega/Lc).
+// The early exit of the reference (max |dx_0| < 1e-14 after a sweep) is taken on the device: a sweep that
+// finds the previous one converged copies x forward. LAST adds the increment to the state
+// (solverUpdateUImplicit, solver.c:1945-1955) and computes the next iteration's primitives.
+// ------------------------------------------------------------------------------------------------
+template <int MODEL, bool LAST>
+__global__ void __launch_bounds__(BLOCK) k_sweep(const __grid_constant__ Prm p, const __grid_constant__ Mesh m,
+                                                 const __grid_constant__ State s, int sweep, int cur)
+{
+    constexpr int NV = Model<MODEL>::NV, NP = Model<MODEL>::NP;
+    if (halted(s)) return;
+    int c = blockIdx.x * BLOCK + threadIdx.x;
+    const int nc = m.nc;
+    bool conv = sweep > 0 && bitsd(s.sc->sweep_max[sweep - 1]) < 1e-14;
+    double dmax = 0.0;
+    if (c < nc) {
+        const double4* xo4 = s.X4[cur];
+        const double* xox = s.Xx[cur];
+        double4* xn4 = s.X4[cur ^ 1];
+        double* xnx = s.Xx[cur ^ 1];
+        double xo[NV], xn[NV];
+        {
+            double4 t = xo4[c];
+            xo[0] = t.x; xo[1] = t.y; xo[2] = t.z; xo[3] = t.w;
+#pragma unroll
+            for (int k = 4; k < NV; k++) xo[k] = xox[(size_t)(k - 4) * nc + c];
+        }
+        if (conv) {
+#pragma unroll
+            for (int k = 0; k < NV; k++) xn[k] = xo[k];
+        } else {
+            double dt = bitsd(s.sc->dtmin_bits) * p.cfl;
+            double D = s.dpart[c] + m.omega[c] / dt;
+            double y[NV];
+#pragma unroll
+            for (int k = 0; k < NV; k++) y[k] = D * xo[k];
+            const int ni = m.nint[c];
+            for (int j = 0; j < ni; j++) {
+                int sf = m.fslot[(size_t)j * nc + c];
+                int f = sf > 0 ? sf - 1 : -sf - 1;
+                int2 e = m.fe[f];
+                int nb = sf > 0 ? e.y : e.x;
+                double xb[NV];
+                double4 t = xo4[nb];
+                xb[0] = t.x; xb[1] = t.y; xb[2] = t.z; xb[3] = t.w;
+#pragma unroll
+                for (int k = 4; k < NV; k++) xb[k] = xox[(size_t)(k - 4) * nc + nb];
+                const double* A = s.blocks + (size_t)j * NV * NV * nc + c;
+#pragma unroll
+                for (int kk = 0; kk < NV; kk++)
+#pragma unroll
+                    for (int nn = 0; nn < NV; nn++) y[kk] += A[(size_t)(kk * NV + nn) * nc] * xb[nn];
+            }
+            double R[NV];
+            {
+                double4 t = s.R4[c];
+                R[0] = t.x; R[1] = t.y; R[2] = t.z; R[3] = t.w;
+#pragma unroll
+                for (int k = 4; k < NV; k++) R[k] = s.Rx[(size_t)(k - 4) * nc + c];
+            }
+            const double w = 2. / 3.;
+#pragma unroll
+            for (int k = 0; k < NV; k++) xn[k] = w * (-R[k] - y[k]) / D + xo[k];
+            dmax = fabs(xn[0] - xo[0]);
+        }
+        xn4[c] = make_double4(xn[0], xn[1], xn[2], xn[3]);
+#pragma unroll
+        for (int k = 4; k < NV; k++) xnx[(size_t)(k - 4) * nc + c] = xn[k];
+        if (LAST) {
+            double U[NV], P[NP];
+            loadU<MODEL>(s, nc, c, U);
+#pragma unroll
+            for (int k = 0; k < NV; k++) U[k] += xn[k];
+            clamp_prim<MODEL>(p, U, P);
+            storeU<MODEL>(s, nc, c, U);
+            storeP<MODEL>(s, nc, c, P);
+        }
+    }
+    if (!conv) {
+        double v = warp_max(dmax);
+        if ((threadIdx.x & 31) == 0) atomicMax(&s.sc->sweep_max[sweep], dbits(v));
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// k_finalize: one block closing an iteration (solverCalcRes, solverCalcCoeff3, history row, flags) and
+// preparing the next step size. mode: 0 RK iteration, 1 implicit iteration, 2 prologue (step size only),
+// 3 residual only (norms).
+// ------------------------------------------------------------------------------------------------
+template <int MODEL>
+__global__ void __launch_bounds__(BLOCK) k_finalize(const __grid_constant__ Prm p, const __grid_constant__ Mesh m,
+                                                    const __grid_constant__ State s, int npart, int nwall,
+                                                    int mode, int hist_cap)
+{
+    constexpr int NV = Model<MODEL>::NV;
+    __shared__ double sh[NV + 4][BLOCK / 32];
+    Scalars* sc = s.sc;
+    if (mode != 2 && mode != 3 && halted(s)) return;
+    double v[NV + 4];
+#pragma unroll
+    for (int k = 0; k < NV + 4; k++) v[k] = 0.0;
+    if (mode != 2) {
+        // contiguous chunks per thread, then a fixed tree: deterministic
+        int per = (npart + BLOCK - 1) / BLOCK;
+        for (int i = threadIdx.x * per; i < min(npart, (int)(threadIdx.x + 1) * per); i++)
+#pragma unroll
+            for (int k = 0; k < NV; k++) v[k] += s.part[(size_t)i * NV + k];
+        int perw = (nwall + BLOCK - 1) / BLOCK;
+        for (int i = threadIdx.x * perw; i < min(nwall, (int)(threadIdx.x + 1) * perw); i++)
+#pragma unroll
+            for (int k = 0; k < 4; k++) v[NV + k] += s.bcoef[(size_t)i * 4 + k];
+    }
+    block_sum<NV + 4>(v, sh);
+    if (threadIdx.x != 0) return;
+    if (mode != 2) {
+        bool bad = false;
+        for (int k = 0; k < NV; k++) {
+            sc->res[k] = sqrt(v[k] / m.nc);
+            if (!isfinite(sc->res[k])) bad = true;
+        }
+        double cxp = v[NV] / p.sref, cyp = v[NV + 1] / p.sref, cxv = v[NV + 2] / p.sref, cyv = v[NV + 3] / p.sref;
+        if (p.axi) {
+            cxp *= 2 * M_PI;
+            cxv *= 2 * M_PI;
+        }
+        sc->coef[0] = cxp; sc->coef[1] = cxv; sc->coef[2] = cyp; sc->coef[3] = cyv;
+        if (mode == 3) return;
+        if (s.hist && sc->hist_row < hist_cap) {
+            double* row = s.hist + (size_t)sc->hist_row * (NV + 4);
+            for (int k = 0; k < NV; k++) row[k] = sc->res[k];
+            row[NV] = cxp; row[NV + 1] = cxv; row[NV + 2] = cyp; row[NV + 3] = cyv;
+        }
+        sc->hist_row++;
+        if (!sc->have_res0) {
+            for (int k = 0; k < NV; k++) sc->res0[k] = sc->res[k];
+            sc->have_res0 = 1;
+        }
+        sc->steps++;
+        if (sc->iter == p.dt_local_n) sc->dt_local = 0;
+        sc->iter++;
+        if (bad) sc->status = 4; // CSU_ERR_NONFINITE
+        if (p.tube) {
+            sc->t += sc->dt * p.stages / 2.0;
+            if (sc->stop_after) sc->done = 1;
+        }
+        if (p.conv_tol > 0 && sc->res[0] <= p.conv_tol * sc->res0[0]) sc->done = 1;
+        for (int k = 0; k < MAX_SWEEPS; k++) sc->sweep_max[k] = 0ULL;
+    }
+    if (mode == 0 || mode == 2) {
+        // solverCalcDt (solver.c:925-950) for the next iteration, from the minimum gathered above
+        double dt = bitsd(sc->dtmin_bits);
+        dt *= p.cfl;
+        if (p.tube && sc->t + dt > p.tmax) {
+            dt = (p.tmax - sc->t);
+            sc->stop_after = 1;
+        }
+        sc->dt = dt;
+    }
+    sc->dtmin_bits = 0x7ff0000000000000ULL;
+}
+
+} // namespace csu

@@ -1,0 +1,76 @@
+/* layout.h -- device data layout built on the host from a csu_mesh_desc (internal). */
+#ifndef CSU_LAYOUT_H
+#define CSU_LAYOUT_H
+
+#include "csu_gpu.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/*
+ * Cells are renumbered along a Hilbert curve through their centroids; interior faces are sorted by their
+ * lower renumbered cell, boundary faces by owner. All per-cell slot arrays are [slot][cell] (4 slots).
+ * Geometry is computed with the reference's expressions so it is bit-identical to what the reference
+ * recomputes on the fly (elementCenter, meshCalcDS, edge midpoints).
+ */
+typedef struct csu_layout {
+    int nc, nf, nb, nv;
+    int* cell_new2old;
+    int* cell_old2new;
+    int* face_new2old;
+    int* face_old2new;
+    int* bface_new2old;
+    int* bface_old2new;
+
+    /* per renumbered cell */
+    int* npts;     /* nodes = edges = neighbour slots                                                 */
+    int* nint;     /* interior faces                                                                  */
+    int* nslot;    /* face slots = interior + boundary faces of the cell                              */
+    int* nei;      /* [4][nc] neighbour (ELEMENT.neiL order): cell id, or nc + boundary face id       */
+    double* wx;    /* [4][nc] least-squares weights: dUx = sum wx (u_nei - u_cell)                     */
+    double* wy;
+    double* ex;    /* [4][nc] edge midpoint minus centroid, edges in node order (limiter, inter)        */
+    double* ey;
+    int* fslot;    /* [4][nc] +-(flux index + 1): interior faces (ELEMENT.f order) then boundary faces  */
+    double* omega;
+    double* sxh;   /* 0.5 * sum |dSx| over the cell edges (solverLocalTimeStep, solver.c:904-914)      */
+    double* syh;
+    double* xc;    /* centroid (elementCenter)                                                        */
+    double* yc;
+    double* wall_d;/* wall distance or NULL                                                           */
+    double* dslat; /* meshCalcDSlateral (axisymmetric pressure source)                                */
+
+    /* per renumbered interior face (orientation of mesh->con) */
+    int* fe0;
+    int* fe1;
+    double* fdsx;  /* meshCalcDS (axisymmetric scaling included)                                      */
+    double* fdsy;
+    double* fds;   /* sqrt(dSx^2 + dSy^2)                                                             */
+    double* r0x;   /* face midpoint minus centroid of e0 / e1                                         */
+    double* r0y;
+    double* r1x;
+    double* r1y;
+    double* fdist; /* centroid distance |x_e1 - x_e0| (viscous terms)                                 */
+
+    /* per renumbered boundary face */
+    int* bown;
+    int* bflag;
+    int* bold;     /* reference (marker-major) id                                                     */
+    double* bdsx;
+    double* bdsy;
+    double* bds;
+    double* bmx;   /* edge midpoint (ghost centre)                                                    */
+    double* bmy;
+
+    double vol_max;/* max omega (limiterUpdate type 0, limiter.c:44-48)                               */
+    int max_npts;
+} csu_layout;
+
+int csu_layout_build(const csu_mesh_desc* m, int axi, csu_layout* L);
+void csu_layout_free(csu_layout* L);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,192 @@
+/*
+ * csu_gpu.h -- C ABI of the B200 residual-and-update engine for CSU cases.
+ *
+ * The reference solver has no plugin API: its seam is the C function interface of solver.h:172-260 and
+ * implicit.h, every function taking a SOLVER* that owns all host arrays. This header replaces the
+ * per-iteration body of solverSolve (solver.c:1864-1907 and the tube loop 1921-1940) -- solverCalcR
+ * (solver.c:685), solverCalcDt (925), solverStepRK (788), implicitCalcD/LUSGS_L/LUSGS_U/CalcDPLUR
+ * (implicit.c:19,274,365,990), solverUpdateUImplicit (solver.c:1945), solverCalcRes (867) and
+ * solverCalcCoeff3 (1342) -- with calls that take plain pointers and sizes.
+ *
+ * Conventions
+ *  - Every entry returns an int status (CSU_OK == 0). The library never calls exit() and never aborts;
+ *    csu_last_error() gives a one-line message for the calling thread's last failure.
+ *  - Host arrays are caller-owned; device arrays are library-owned (allocated in csu_create, freed in
+ *    csu_destroy). All host-side state arrays are in the reference's numbering (cell ii of
+ *    mesh->elemL, face of mesh->con, boundary elements marker-major), whatever order the device uses.
+ *  - Conserved state U and residual R are "[var][cell]" flat arrays: U[k*ncells + i] == solver->U[k][i].
+ *  - One context per host thread; calls on one context are not re-entrant.
+ */
+#ifndef CSU_GPU_H
+#define CSU_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (the reference prints and exit(0)s instead: input.c:136-140, flux.c:38-42) ---- */
+#define CSU_OK 0
+#define CSU_ERR_INPUT 1       /* missing/invalid keyword, malformed SU2 file, bad argument          */
+#define CSU_ERR_IO 2          /* file cannot be opened/written                                        */
+#define CSU_ERR_OOM 3         /* device allocation failed or the request exceeds the memory budget   */
+#define CSU_ERR_NONFINITE 4   /* a residual or state value became NaN/Inf on the device              */
+#define CSU_ERR_DIVERGED 5    /* residual grew past the divergence threshold                          */
+#define CSU_ERR_CANCELLED 6   /* a serving request was cancelled                                      */
+#define CSU_ERR_CUDA 7        /* a CUDA runtime call failed                                           */
+#define CSU_ERR_UNSUPPORTED 8 /* setting the engine does not implement                               */
+#define CSU_ERR_STATE 9       /* call made in the wrong state (e.g. before csu_set_state)            */
+#define CSU_ERR_NO_DEVICE 10  /* no CUDA device / extension missing                                   */
+
+/* flux schemes, fluxChoice (flux.c:14-46) */
+#define CSU_FLUX_ROE 0
+#define CSU_FLUX_AUSM 1
+#define CSU_FLUX_AUSMDV 2
+#define CSU_FLUX_AUSMPUP 3
+#define CSU_FLUX_AUSMPUP2 4
+
+/* boundary flags, boundaryChoice (boundary.c:479-511) */
+#define CSU_BC_SYMMETRY 0
+#define CSU_BC_INLET 1
+#define CSU_BC_OUTLET 2
+#define CSU_BC_WALL 3
+#define CSU_BC_WALLT 4
+
+/* time schemes, solverTimeSchemeChoice (solver.c:1957-1981) */
+#define CSU_TS_RK 0
+#define CSU_TS_LUSGS 1
+#define CSU_TS_DPLUR 2
+
+/* Scalar settings of one solve: the SOLVER fields of solver.h:86-170 that the hot path reads. */
+typedef struct csu_config {
+    int nvar;          /* 4 Euler/laminar, 5 SA, 6 SST (solver.c:1789-1798)                      */
+    int order;         /* 1 or 2                                                                 */
+    int flux;          /* CSU_FLUX_*                                                             */
+    int stages;        /* RK stages 1, 3, 4, 5 (solver.c:788-840)                                */
+    int time_scheme;   /* CSU_TS_*                                                               */
+    int n_linear;      /* DPLUR sweeps (Nlinear, default 20)                                     */
+    int dt_local;      /* local time step for RK (dtLocal)                                       */
+    int dt_local_n;    /* iteration after which dtLocal switches off (dtLocalN, -1 = never)      */
+    int laminar, sa, sa_cc, sst, sst_trans, axisymmetric, turb1order, visc_blazek, tp;
+    int limiter_type;  /* 0: K^3 (omega/omega_max)^1.5 q_inf^2, 1: (K (max-min))^2 (limiter.c)  */
+    int tube;          /* unsteady shock-tube mode (solver.c:1912)                               */
+    double limiter_k;  /* limK                                                                   */
+    double cfl, w_imp, r_lim, p_out, t_wall, sref, turb_ratio, e_fix, pr, pr_t;
+    double gamma, gas_r;                  /* 1.4, 287.0530 (solver.c:1425)                       */
+    double pin[7];                        /* inlet primitives r,u,v,p,T,(nt | k,w) CONDITION.Pin */
+    double uin[6];                        /* inlet conserved state CONDITION.Uin                  */
+    double mach_inf;                      /* CONDITION.mach (AUSM+up M_inf)                       */
+    double inlet_p, inlet_t;              /* CONDITION.p, CONDITION.T                             */
+    double sst_l, k_factor, o_factor, o_wall_factor;
+} csu_config;
+
+/*
+ * The mesh as meshInit (mesh.c:115-266) leaves it, as plain arrays. A caller holding the reference's
+ * MESH* fills it directly; csu_case_load builds the same arrays from a case folder.
+ */
+typedef struct csu_mesh_desc {
+    int n_points;
+    const double* xy;          /* 2 per point (mesh->p)                                           */
+    int n_cells;
+    const int* cell_npts;      /* 3 or 4 (ELEMENT.Np)                                             */
+    const int* cell_nodes;     /* 4 per cell, counter-clockwise after mesh.c:222-242, -1 padded   */
+    int n_faces;               /* interior faces (mesh->Ncon)                                     */
+    const int* con;            /* 4 per face: e0, e1, p0, p1 (mesh->con, face order of mesh.c:1172) */
+    const int* cell_nint;      /* interior faces of the cell (ELEMENT.neiN after meshCalcFaces)    */
+    const int* cell_faces;     /* 4 per cell: +(f+1) owner / -(f+1) neighbour (ELEMENT.f)          */
+    const int* cell_nei;       /* 4 per cell in ELEMENT.neiL order: >=0 cell, <0 -(1+boundary face) */
+    int n_markers;
+    const int* marker_nbf;     /* boundary faces per marker (MESHBC.Nelem)                        */
+    const int* marker_flag;    /* CSU_BC_* per marker (MESHBC.flagBC)                             */
+    int n_bfaces;              /* sum of marker_nbf                                               */
+    const int* bface;          /* 3 per boundary face, marker-major: p0, p1 (mesh.c:987), owner   */
+    const double* wall_dist;   /* per cell (ELEMENT.d, sa.c:703) or NULL                          */
+} csu_mesh_desc;
+
+/* Per-iteration record, the quantities solverSolve prints and writes to convergence.csv
+ * (solver.c:1891-1906): hist[it*(nvar+4) + k] = res[k], then Cx_p, Cx_v, Cy_p, Cy_v. */
+#define CSU_HIST_STRIDE(nvar) ((nvar) + 4)
+
+typedef struct csu_ctx csu_ctx;
+typedef struct csu_case csu_case;
+
+/* ------------------------------------------------------------------------------------------------
+ * Host front end (C): a case folder as the reference reads it.
+ * ---------------------------------------------------------------------------------------------- */
+
+/* Parse <wd>input.dat (input.c:7-95), read <wd>mesh.su2 and build the connectivity
+ * (meshInit, mesh.c:115-266), apply solverSetData/solverInit (solver.c:1403-1834) and the initial
+ * state of solverInitDomain (solver.c:1660-1726: freestream, tube or restart.csv). Replaces
+ * solverInit (solver.c:1728) minus device work. Wall distance (sa.c:703-793) is computed when sa/sst. */
+int csu_case_load(const char* wd, csu_case** out);
+/* Same from in-memory file contents (no file system). */
+int csu_case_load_mem(const char* input_dat, const char* mesh_su2, const char* restart_csv, csu_case** out);
+int csu_case_mesh(const csu_case* c, csu_mesh_desc* out);         /* views into the case          */
+int csu_case_config(const csu_case* c, csu_config* out);
+int csu_case_initial_state(const csu_case* c, double* U);         /* nvar*ncells, [var][cell]     */
+int csu_case_get_int(const csu_case* c, const char* keyword, int* out);        /* inputGetValue  */
+int csu_case_get_double(const csu_case* c, const char* keyword, double* out);
+int csu_case_marker_name(const csu_case* c, int marker, char* out, int cap);
+void csu_case_free(csu_case* c);
+
+/* ------------------------------------------------------------------------------------------------
+ * Device engine.
+ * ---------------------------------------------------------------------------------------------- */
+
+/* Build the device layout (renumbered cells, face streams, geometry, least-squares weights) and
+ * allocate all device state on the current CUDA device. The DPLUR increment starts at zero like
+ * implicitInitDPLUR (implicit.c:649-656). */
+int csu_create(const csu_mesh_desc* mesh, const csu_config* cfg, csu_ctx** out);
+void csu_destroy(csu_ctx* ctx);
+
+/* Upload/download the conserved state, [var][cell] in reference cell order. */
+int csu_set_state(csu_ctx* ctx, const double* U);
+int csu_get_state(csu_ctx* ctx, double* U);
+/* Same with the reference's row pointers: U[k][i] (solver->U). */
+int csu_set_state_rows(csu_ctx* ctx, const double* const* U);
+int csu_get_state_rows(csu_ctx* ctx, double* const* U);
+
+/* One residual evaluation solverCalcR(solver, solver->U) (solver.c:685) on the device, including its
+ * write-back clamps into U (solver.c:1163-1211). R (nullable) receives [var][cell]. */
+int csu_residual(csu_ctx* ctx, double* R);
+
+/* n iterations of the steady loop of solverSolve (solver.c:1864-1906) on the device; it0 is the
+ * iteration counter of the first one (dtLocalN uses it). hist (nullable) gets n rows of
+ * CSU_HIST_STRIDE(nvar) doubles. Returns CSU_ERR_NONFINITE if the state became non-finite. */
+int csu_iterate(csu_ctx* ctx, int n, int it0, double* hist);
+
+/* The unsteady tube loop (solver.c:1912-1942) up to tmax; returns steps taken and final time. */
+int csu_tube_run(csu_ctx* ctx, double tmax, int* steps, double* t_final);
+
+/* Debug/parity views of the last residual evaluation, reference layouts:
+ *  CSU_DUMP_P       ncells*(nvar+1) [cell][k]   cell primitives ELEMENT.P
+ *  CSU_DUMP_GHOST_P nbfaces*(nvar+1)            ghost primitives of boundary elements
+ *  CSU_DUMP_GRAD    2*nvar*ncells               dPx rows then dPy rows ([k][cell])
+ *  CSU_DUMP_PHI     nvar*ncells                 limiter phi
+ *  CSU_DUMP_FACEFLUX nvar*nfaces                faceFlux [k][face]
+ *  CSU_DUMP_R       nvar*ncells                 residual
+ *  CSU_DUMP_D       ncells                      implicit diagonal D (after an implicit iteration)
+ *  CSU_DUMP_DTL     ncells                      dtL (local steps, or Omega/Lc for implicit)
+ *  CSU_DUMP_DW      nvar*ncells                 last implicit increment dW1
+ *  CSU_DUMP_BLOCKS  ncells*4*nvar*nvar          DPLUR blocks [cell][slot][row][col], slots in ELEMENT.f order */
+#define CSU_DUMP_P 1
+#define CSU_DUMP_GHOST_P 2
+#define CSU_DUMP_GRAD 3
+#define CSU_DUMP_PHI 4
+#define CSU_DUMP_FACEFLUX 5
+#define CSU_DUMP_R 6
+#define CSU_DUMP_D 7
+#define CSU_DUMP_DTL 8
+#define CSU_DUMP_DW 9
+#define CSU_DUMP_BLOCKS 10
+int csu_dump(csu_ctx* ctx, int what, double* out);
+
+/* Counters of the engine: kernels launched since creation, device bytes held. */
+int csu_stats(csu_ctx* ctx, long long* kernel_launches, long long* device_bytes);
+
+const char* csu_last_error(void);
+const char* csu_strerror(int status);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

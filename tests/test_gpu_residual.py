@@ -1,0 +1,169 @@
+"""CUDA path vs the reference solver (oracle/_ref) on the reference's own example cases.
+
+Bar (per cell, per variable): one residual evaluation within 1e-12 of the cell's flux scale
+(sum of |face fluxes| of the cell plus |R|), the residual history of the first iterations within 1e-9
+relative, primitives and ghost states bit for bit.
+"""
+import numpy as np
+import pytest
+
+import casekit
+
+pytestmark = pytest.mark.gpu
+
+RTOL_R = 1e-12
+RTOL_HIST = 1e-9
+
+
+def _ref(wd):
+    from oracle.refharness import Ref, available
+    if not available():
+        pytest.skip("reference build oracle/_ref missing")
+    return Ref(wd)
+
+
+def _engine(wd):
+    import csu_b200
+    case = csu_b200.Case.load(wd)
+    return csu_b200.Engine(case), case
+
+
+def _cell_scale(case, ff, R):
+    nc, nv = case.n_cells, R.shape[0]
+    S = np.abs(R).copy()
+    for j in range(4):
+        sf = case.cell_faces[:, j]
+        used = (np.arange(4)[j] < case.cell_nint)
+        idx = np.where(used)[0]
+        f = np.abs(sf[idx]) - 1
+        S[:, idx] += np.abs(ff[:, f])
+    return S + 1e-300
+
+
+def _rel(a, b):
+    return np.max(np.abs(a - b) / (np.abs(b) + 1e-300))
+
+
+STEADY = ["caseChannel", "caseCylinder", "caseCylinderAxi", "caseDiamond", "caseWedge", "caseWedgeAxi",
+          "caseWedgeQuad"]
+
+
+@pytest.mark.parametrize("name", casekit.INVISCID)
+def test_residual_parity(native, name):
+    wd = casekit.materialize(name, casekit.GOLDEN_OVERRIDES.get(name, {}))
+    eng, case = _engine(wd)
+    ref = _ref(wd)
+    R_ref = ref.calc_R()
+    R = eng.residual()
+    ff_ref = ref.faceflux()
+    S = _cell_scale(case, ff_ref, R_ref)
+    err = np.max(np.abs(R - R_ref) / S)
+    assert err < RTOL_R, err
+    P = eng.dump("P")
+    assert np.array_equal(P, ref.P())
+    gp = eng.dump("GHOST_P")
+    assert np.array_equal(gp, ref.ghost_P())
+    ff = eng.dump("FACEFLUX")
+    fs = np.abs(ff_ref).max(axis=1, keepdims=True) + 1e-300
+    assert np.max(np.abs(ff - ff_ref) / fs) < RTOL_R
+
+
+@pytest.mark.parametrize("flux", ["ROE", "AUSM", "AUSMDV", "AUSMpup", "AUSMpup2"])
+@pytest.mark.parametrize("order", [1, 2])
+@pytest.mark.parametrize("name", ["caseCylinder", "caseWedgeQuad"])
+def test_flux_schemes(native, name, flux, order):
+    wd = casekit.materialize(name, {"flux": flux, "order": str(order)})
+    eng, case = _engine(wd)
+    ref = _ref(wd)
+    # a non-uniform state: a few RK iterations of the reference
+    ref.iterate(3)
+    U = ref.get_U()
+    eng.set_state(U)
+    R_ref = ref.calc_R()
+    R = eng.residual()
+    S = _cell_scale(case, ref.faceflux(), R_ref)
+    assert np.max(np.abs(R - R_ref) / S) < RTOL_R
+    if order == 2:
+        g = eng.dump("GRAD")
+        gr = ref.grad()
+        gs = np.abs(gr).max(axis=2, keepdims=True) + 1e-300
+        assert np.max(np.abs(g - gr) / gs) < 1e-11
+        ph = eng.dump("PHI")
+        assert np.max(np.abs(ph - ref.phi())) < 1e-10
+
+
+@pytest.mark.parametrize("name", STEADY)
+def test_history_parity(native, name):
+    wd = casekit.materialize(name, casekit.GOLDEN_OVERRIDES.get(name, {}))
+    eng, case = _engine(wd)
+    ref = _ref(wd)
+    n = 20
+    h_ref = ref.iterate(n)
+    h = eng.iterate(n)
+    assert h.shape == h_ref.shape
+    nv = case.nvar
+    assert _rel(h[:, :nv], h_ref[:, :nv]) < RTOL_HIST
+    cs = np.abs(h_ref[:, nv:]).max() + 1e-300
+    assert np.max(np.abs(h[:, nv:] - h_ref[:, nv:])) / cs < RTOL_HIST
+    U, U_ref = eng.get_state(), ref.get_U()
+    us = np.abs(U_ref).max(axis=1, keepdims=True)
+    assert np.max(np.abs(U - U_ref) / us) < RTOL_HIST
+
+
+@pytest.mark.parametrize("name,scheme", [("caseCylinder", "DPLUR"), ("caseDiamond", "DPLUR"),
+                                         ("caseWedgeQuad", "RK")])
+def test_scheme_variants(native, name, scheme):
+    kv = {"timeScheme": scheme}
+    if scheme == "DPLUR":
+        kv.update({"Nlinear": "4", "CFL": "5.0"})
+    else:
+        kv.update({"stages": "3", "dtLocal": "1", "dtLocalN": "5"})
+    wd = casekit.materialize(name, kv)
+    eng, case = _engine(wd)
+    ref = _ref(wd)
+    n = 12
+    h_ref = ref.iterate(n)
+    h = eng.iterate(n)
+    nv = case.nvar
+    assert _rel(h[:, :nv], h_ref[:, :nv]) < RTOL_HIST
+    U, U_ref = eng.get_state(), ref.get_U()
+    us = np.abs(U_ref).max(axis=1, keepdims=True)
+    assert np.max(np.abs(U - U_ref) / us) < RTOL_HIST
+
+
+def test_dplur_pieces(native):
+    wd = casekit.materialize("caseWedge", casekit.GOLDEN_OVERRIDES["caseWedge"])
+    eng, case = _engine(wd)
+    ref = _ref(wd)
+    ref.iterate(2)
+    eng.iterate(2)
+    # one more iteration on both, then compare the implicit operator pieces of that iteration
+    U = ref.get_U()
+    eng.set_state(U)
+    R_ref = ref.calc_R()
+    D_ref, dtl_ref = ref.implicit_D()
+    A_ref = ref.implicit_A()
+    eng.iterate(1)
+    D, dtl = eng.dump("D"), eng.dump("DTL")
+    assert _rel(dtl, dtl_ref) < 1e-12
+    assert _rel(D, D_ref) < 1e-12
+    A = eng.dump("BLOCKS")
+    for c in range(0, case.n_cells, 97):
+        ni = case.cell_nint[c]
+        a, b = A[c, :ni], A_ref[c, :ni]
+        assert np.max(np.abs(a - b)) <= 1e-12 * (np.abs(b).max() + 1e-300)
+
+
+@pytest.mark.parametrize("name", ["caseSod", "caseSodRef"])
+def test_tube(native, name):
+    wd = casekit.materialize(name, {})
+    eng, case = _engine(wd)
+    ref = _ref(wd)
+    tmax = 0.002
+    steps_ref, t_ref = ref.tube_run(tmax)
+    steps, t = eng.tube_run(tmax)
+    assert steps == steps_ref
+    assert abs(t - t_ref) <= 1e-12 * t_ref
+    U, U_ref = eng.get_state(), ref.get_U()
+    us = np.abs(U_ref).max(axis=1, keepdims=True)
+    assert np.max(np.abs(U - U_ref) / us) < RTOL_HIST
