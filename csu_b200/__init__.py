@@ -90,6 +90,8 @@ def lib():
         L.csu_tube_run.argtypes = [vp, C.c_double, ip, dp]
         L.csu_dump.argtypes = [vp, C.c_int, vp]
         L.csu_stats.argtypes = [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
+        L.csu_set_stream.argtypes = [vp, vp]
+        L.csu_time_kernels.argtypes = [vp, C.c_int, dp, ip]
         _lib = L
     return _lib
 
@@ -221,6 +223,17 @@ class Engine:
         out = np.zeros(shapes[what])
         _check(lib().csu_dump(self._h, DUMP[what], _ptr(out)))
         return out
+
+    def set_stream(self, stream):
+        """Run on a caller's cudaStream_t (an int handle, e.g. torch.cuda.Stream().cuda_stream); None resets."""
+        _check(lib().csu_set_stream(self._h, C.c_void_p(stream) if stream else None))
+
+    def time_kernels(self, iters):
+        """Device time per kernel kind over `iters` iterations (the state advances)."""
+        ms = (C.c_double * 8)()
+        cnt = (C.c_int * 8)()
+        _check(lib().csu_time_kernels(self._h, iters, ms, cnt))
+        return {"ms": list(ms), "count": list(cnt)}
 
     def stats(self):
         a, b = C.c_longlong(), C.c_longlong()

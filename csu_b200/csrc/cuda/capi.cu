@@ -53,7 +53,30 @@ struct csu_ctx {
     cudaGraphExec_t graph = nullptr;
     int graph_iters = 0;
     int have_debug = 0;
+    cudaStream_t own_stream = nullptr;
+    // kernel timing (csu_time_kernels): an event after every launch, tagged with the kernel kind
+    bool timing = false;
+    std::vector<cudaEvent_t> ev;
+    std::vector<int> ev_kind;
+    size_t ev_used = 0;
 };
+
+// kinds of csu_time_kernels
+enum { KPRIM = 0, KGRAD, KFLUX, KRK, KIMPL, KSWEEP, KFIN, KRESID, KCOUNT };
+
+static void tmark(csu_ctx* x, int kind)
+{
+    if (!x->timing) return;
+    if (x->ev_used == x->ev.size()) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        x->ev.push_back(e);
+        x->ev_kind.push_back(kind);
+    }
+    x->ev_kind[x->ev_used] = kind;
+    cudaEventRecord(x->ev[x->ev_used], x->stream);
+    x->ev_used++;
+}
 
 static int cuda_fail(cudaError_t e, const char* what)
 {
@@ -93,6 +116,11 @@ static void plan(csu_ctx* x, Arena& a)
     m.nei = carve<int>(a, c4);
     m.wx = carve<double>(a, c4);
     m.wy = carve<double>(a, c4);
+    m.ldx = carve<double>(a, c4);
+    m.ldy = carve<double>(a, c4);
+    m.lm = carve<unsigned long long>(a, c4);
+    m.les = carve<int>(a, c4);
+    m.lrv = carve<unsigned long long>(a, nc);
     m.ex = carve<double>(a, c4);
     m.ey = carve<double>(a, c4);
     m.fslot = carve<int>(a, c4);
@@ -179,6 +207,11 @@ static int upload_mesh(csu_ctx* x)
     CK(up(m.nei, L.nei, sizeof(int) * c4));
     CK(up(m.wx, L.wx, sizeof(double) * c4));
     CK(up(m.wy, L.wy, sizeof(double) * c4));
+    CK(up(m.ldx, L.ldx, sizeof(double) * c4));
+    CK(up(m.ldy, L.ldy, sizeof(double) * c4));
+    CK(up(m.lm, L.lm, sizeof(unsigned long long) * c4));
+    CK(up(m.les, L.les, sizeof(int) * c4));
+    CK(up(m.lrv, L.lrv, sizeof(unsigned long long) * nc));
     CK(up(m.ex, L.ex, sizeof(double) * c4));
     CK(up(m.ey, L.ey, sizeof(double) * c4));
     CK(up(m.fslot, L.fslot, sizeof(int) * c4));
@@ -252,6 +285,9 @@ static void fill_params(csu_ctx* x)
     p.sst_b1 = 0.075;
     p.o_wall_factor = c.o_wall_factor;
     p.tmax = 0;
+    // exact x87 gradients unless CSU_LSQ_FAST=1 (FP64 weights: faster, last-bit differences)
+    const char* fast = getenv("CSU_LSQ_FAST");
+    p.lsq_exact = (fast && fast[0] == '1') ? 0 : 1;
     p.conv_tol = 0;
 }
 
@@ -344,7 +380,8 @@ extern "C" int csu_create(const csu_mesh_desc* md, const csu_config* cfg, csu_ct
     x->arena.used = 0;
     plan(x, x->arena);
     e = cudaMemset(x->arena.base, 0, bytes);
-    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&x->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&x->own_stream, cudaStreamNonBlocking);
+    x->stream = x->own_stream;
     if (e != cudaSuccess) {
         cudaFree(x->arena.base);
         csu_layout_free(&x->L);
@@ -373,7 +410,8 @@ extern "C" void csu_destroy(csu_ctx* x)
     if (!x) return;
     if (x->graph) cudaGraphExecDestroy(x->graph);
     if (x->st.hist) cudaFree(x->st.hist);
-    if (x->stream) cudaStreamDestroy(x->stream);
+    for (cudaEvent_t e : x->ev) cudaEventDestroy(e);
+    if (x->own_stream) cudaStreamDestroy(x->own_stream);
     if (x->arena.base) cudaFree(x->arena.base);
     csu_layout_free(&x->L);
     delete x;
@@ -440,6 +478,7 @@ static void launch_grad(csu_ctx* x, bool dbg)
     if (dbg) k_grad<MODEL, true><<<x->gb_c, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st);
     else k_grad<MODEL, false><<<x->gb_c, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st);
     x->launches++;
+    tmark(x, KGRAD);
 }
 
 template <int MODEL>
@@ -448,6 +487,7 @@ static void launch_flux(csu_ctx* x, int coef)
     k_flux<MODEL><<<x->gb_fi + x->gb_fb, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st, x->gb_fi, x->d_wall_rank,
                                                                  coef);
     x->launches++;
+    tmark(x, KFLUX);
 }
 
 template <int MODEL>
@@ -455,6 +495,7 @@ static void launch_finalize(csu_ctx* x, int mode)
 {
     k_finalize<MODEL><<<1, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st, x->gb_c, x->nwall, mode, x->hist_cap);
     x->launches++;
+    tmark(x, KFIN);
 }
 
 template <int MODEL>
@@ -463,6 +504,7 @@ static void launch_prologue(csu_ctx* x)
     int rk = x->cfg.time_scheme == CSU_TS_RK;
     k_prim<MODEL><<<x->gb_c, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st, rk);
     x->launches++;
+    tmark(x, KPRIM);
     launch_finalize<MODEL>(x, 2);
 }
 
@@ -479,6 +521,7 @@ static void launch_iteration(csu_ctx* x)
             if (last) k_rk<MODEL, true><<<x->gb_c, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st, x->rk[sgi]);
             else k_rk<MODEL, false><<<x->gb_c, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st, x->rk[sgi]);
             x->launches++;
+            tmark(x, KRK);
         }
         launch_finalize<MODEL>(x, 0);
     } else {
@@ -486,11 +529,13 @@ static void launch_iteration(csu_ctx* x)
         launch_flux<MODEL>(x, 1);
         k_impl<MODEL, true><<<x->gb_c, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st);
         x->launches++;
+        tmark(x, KIMPL);
         for (int m = 0; m < c.n_linear; m++) {
             if (m == c.n_linear - 1)
                 k_sweep<MODEL, true><<<x->gb_c, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st, m, x->xcur);
             else k_sweep<MODEL, false><<<x->gb_c, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st, m, x->xcur);
             x->launches++;
+            tmark(x, KSWEEP);
             x->xcur ^= 1;
         }
         launch_finalize<MODEL>(x, 1);
@@ -790,5 +835,45 @@ extern "C" int csu_stats(csu_ctx* x, long long* launches, long long* bytes)
 {
     if (launches) *launches = x->launches;
     if (bytes) *bytes = (long long)x->arena.size + (long long)x->hist_cap * (x->nv + 4) * 8;
+    return CSU_OK;
+}
+
+extern "C" int csu_set_stream(csu_ctx* x, void* stream)
+{
+    if (!x) return CSU_ERR_INPUT;
+    CK(cudaStreamSynchronize(x->stream));
+    x->stream = stream ? (cudaStream_t)stream : x->own_stream;
+    return CSU_OK;
+}
+
+extern "C" int csu_time_kernels(csu_ctx* x, int iters, double* ms, int* count)
+{
+    if (!x || iters < 1) return CSU_ERR_INPUT;
+    int st;
+    for (int k = 0; k < CSU_K_COUNT; k++) {
+        ms[k] = 0.0;
+        count[k] = 0;
+    }
+    if (!x->prepared) {
+        Scalars h;
+        if ((st = run_iterations(x, 1, 0, &h))) return st;
+    }
+    CK(cudaStreamSynchronize(x->stream));
+    x->timing = true;
+    x->ev_used = 0;
+    tmark(x, -1);
+    for (int i = 0; i < iters; i++) DISPATCH(launch_iteration, x);
+    x->timing = false;
+    if ((st = check_launch("timed iterations"))) return st;
+    CK(cudaStreamSynchronize(x->stream));
+    for (size_t i = 1; i < x->ev_used; i++) {
+        float t = 0.f;
+        CK(cudaEventElapsedTime(&t, x->ev[i - 1], x->ev[i]));
+        int k = x->ev_kind[i];
+        if (k >= 0 && k < CSU_K_COUNT) {
+            ms[k] += t;
+            count[k]++;
+        }
+    }
     return CSU_OK;
 }

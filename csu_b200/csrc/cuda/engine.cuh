@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include "physics.cuh"
+#include "ext80.cuh"
 
 namespace csu {
 
@@ -21,6 +22,7 @@ struct Prm {
     Gas gas;
     int nc, nf, nb;
     int order, scheme, laminar, sa, sst, axi, turb1order, limiter_type, stages, dt_local_n, tube, n_linear;
+    int lsq_exact;      // gradients with the reference's x87 rounding (1) or precomputed FP64 weights (0)
     double lim_k, vol_max, e_fix, r_lim, p_out, t_wall, pr, pr_t, w_imp, cfl, sigma, mach_inf, sref;
     double pin[7];
     double pref20[6];   // limiterUpdate type 0 reference squares (limiter.c:49-59)
@@ -60,6 +62,11 @@ struct Mesh {
     const double* wy;
     const double* ex;
     const double* ey;
+    const double* ldx;              // least squares: neighbour centre minus centroid
+    const double* ldy;
+    const unsigned long long* lm;   // [4][nc] x87 significands of a, b, c, det
+    const int* les;                 // [4][nc] exponent << 1 | sign
+    const unsigned long long* lrv;  // reciprocal of det's significand
     const int* fslot;
     const double* omega;
     const double* sxh;

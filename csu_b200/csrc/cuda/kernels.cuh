@@ -68,13 +68,17 @@ __global__ void __launch_bounds__(BLOCK) k_grad(const __grid_constant__ Prm p, c
     double P0[NP];
     loadP<MODEL>(s, nc, c, P0);
     double gx[NV], gy[NV], qmin[NV], qmax[NV];
+    X80 XA[NV], XB[NV];
 #pragma unroll
     for (int kk = 0; kk < NV; kk++) {
         gx[kk] = 0.0;
         gy[kk] = 0.0;
         qmin[kk] = P0[slot2p(kk)];
         qmax[kk] = P0[slot2p(kk)];
+        XA[kk] = x80_zero(0);
+        XB[kk] = x80_zero(0);
     }
+    const bool exact = p.lsq_exact != 0;
     const int np = m.npts[c];
     const double dw = m.wall_d ? m.wall_d[c] : 0.0;
 #pragma unroll
@@ -93,15 +97,47 @@ __global__ void __launch_bounds__(BLOCK) k_grad(const __grid_constant__ Prm p, c
                     for (int k = 0; k < NP; k++) s.dbg_ghost[(size_t)bo * NP + k] = Pn[k];
                 }
             }
-            double wxj = m.wx[(size_t)j * nc + c], wyj = m.wy[(size_t)j * nc + c];
+            if (exact) {
+                // solverCalcGrad3 (solver.c:1063-1070): double products summed in long double
+                double dxj = m.ldx[(size_t)j * nc + c], dyj = m.ldy[(size_t)j * nc + c];
 #pragma unroll
-            for (int kk = 0; kk < NV; kk++) {
-                double du = Pn[slot2p(kk)] - P0[slot2p(kk)];
-                gx[kk] += wxj * du;
-                gy[kk] += wyj * du;
-                qmax[kk] = fmax(qmax[kk], Pn[slot2p(kk)]);
-                qmin[kk] = fmin(qmin[kk], Pn[slot2p(kk)]);
+                for (int kk = 0; kk < NV; kk++) {
+                    double du = Pn[slot2p(kk)] - P0[slot2p(kk)];
+                    XA[kk] = x80_add(XA[kk], x80_from_double(dxj * du));
+                    XB[kk] = x80_add(XB[kk], x80_from_double(dyj * du));
+                    qmax[kk] = fmax(qmax[kk], Pn[slot2p(kk)]);
+                    qmin[kk] = fmin(qmin[kk], Pn[slot2p(kk)]);
+                }
+            } else {
+                double wxj = m.wx[(size_t)j * nc + c], wyj = m.wy[(size_t)j * nc + c];
+#pragma unroll
+                for (int kk = 0; kk < NV; kk++) {
+                    double du = Pn[slot2p(kk)] - P0[slot2p(kk)];
+                    gx[kk] += wxj * du;
+                    gy[kk] += wyj * du;
+                    qmax[kk] = fmax(qmax[kk], Pn[slot2p(kk)]);
+                    qmin[kk] = fmin(qmin[kk], Pn[slot2p(kk)]);
+                }
             }
+        }
+    }
+    if (exact) {
+        // dUx = (c A - b B) / (a c - b b), dUy = (-b A + a B) / (a c - b b) in long double (solver.c:1072-1073)
+        X80 K[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            int es = m.les[(size_t)q * nc + c];
+            K[q].m = m.lm[(size_t)q * nc + c];
+            K[q].e = es >> 1;
+            K[q].s = es & 1;
+        }
+        unsigned long long rv = m.lrv[c];
+#pragma unroll
+        for (int kk = 0; kk < NV; kk++) {
+            X80 nx = x80_add(x80_mul(K[2], XA[kk]), x80_neg(x80_mul(K[1], XB[kk])));
+            X80 ny = x80_add(x80_mul(x80_neg(K[1]), XA[kk]), x80_mul(K[0], XB[kk]));
+            gx[kk] = x80_to_double(x80_div_pre(nx, K[3], rv));
+            gy[kk] = x80_to_double(x80_div_pre(ny, K[3], rv));
         }
     }
     double phi[NV];

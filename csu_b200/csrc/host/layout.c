@@ -9,8 +9,10 @@
  *
  * Geometry that the reference recomputes in every loop (elementCenter 28% of its run time, meshCalcDS,
  * midpoints) is evaluated once here with the same expressions, so the device reads bit-identical values.
- * The least-squares normal equations of solverCalcGrad3 (solver.c:1031-1074, long double sums) are
- * folded into per-neighbour weights, evaluated in long double and rounded once.
+ * The least-squares normal equations of solverCalcGrad3 (solver.c:1031-1074) depend only on geometry: their
+ * long double coefficients a, b, c and determinant are evaluated here exactly as the reference does (this
+ * host's long double is the same x87 format) and handed to the device's exact extended-precision model,
+ * together with per-neighbour weights for the faster, non-exact gradient variant.
  */
 #include <stdlib.h>
 #include <string.h>
@@ -71,6 +73,28 @@ static unsigned long long hilbert_key(unsigned x, unsigned y)
     return d;
 }
 
+/* x87 long double as significand (bit 63 set) and exponent<<1|sign, the device's ext80 format */
+static void split_ld(long double v, unsigned long long* m, int* es)
+{
+    if (v == 0) {
+        *m = 0;
+        *es = signbit(v) ? 1 : 0;
+        return;
+    }
+    int e;
+    long double f = frexpl(fabsl(v), &e);
+    *m = (unsigned long long)ldexpl(f, 64);
+    *es = ((e - 64) * 2) | (v < 0 ? 1 : 0);
+}
+
+/* floor((2^128 - 1) / d) - 2^64 for a normalised d (invariant-divisor reciprocal) */
+static unsigned long long recip64(unsigned long long d)
+{
+    if (d == 0) return 0;
+    unsigned __int128 all = ~(unsigned __int128)0;
+    return (unsigned long long)(all / d - ((unsigned __int128)1 << 64));
+}
+
 typedef struct {
     unsigned long long key;
     int id;
@@ -90,7 +114,7 @@ void csu_layout_free(csu_layout* L)
                     L->bface_old2new, L->npts, L->nint, L->nslot, L->nei, L->wx, L->wy, L->ex, L->ey,
                     L->fslot, L->omega, L->sxh, L->syh, L->xc, L->yc, L->wall_d, L->dslat, L->fe0, L->fe1,
                     L->fdsx, L->fdsy, L->fds, L->r0x, L->r0y, L->r1x, L->r1y, L->fdist, L->bown, L->bflag,
-                    L->bold, L->bdsx, L->bdsy, L->bds, L->bmx, L->bmy};
+                    L->bold, L->bdsx, L->bdsy, L->bds, L->bmx, L->bmy, L->ldx, L->ldy, L->lm, L->les, L->lrv};
     for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); i++) free(ptrs[i]);
     memset(L, 0, sizeof(*L));
 }
@@ -109,6 +133,7 @@ int csu_layout_build(const csu_mesh_desc* m, int axi, csu_layout* L)
     ALLOC(L->bface_new2old, nb); ALLOC(L->bface_old2new, nb);
     ALLOC(L->npts, nc); ALLOC(L->nint, nc); ALLOC(L->nslot, nc); ALLOC(L->nei, c4);
     ALLOC(L->wx, c4); ALLOC(L->wy, c4); ALLOC(L->ex, c4); ALLOC(L->ey, c4); ALLOC(L->fslot, c4);
+    ALLOC(L->ldx, c4); ALLOC(L->ldy, c4); ALLOC(L->lm, c4); ALLOC(L->les, c4); ALLOC(L->lrv, nc);
     ALLOC(L->omega, nc); ALLOC(L->sxh, nc); ALLOC(L->syh, nc); ALLOC(L->xc, nc); ALLOC(L->yc, nc);
     ALLOC(L->dslat, nc);
     if (m->wall_dist) ALLOC(L->wall_d, nc);
@@ -278,7 +303,12 @@ int csu_layout_build(const csu_mesh_desc* m, int axi, csu_layout* L)
             cc += dy[j] * dy[j];
         }
         long double det = a * cc - bb * bb;
+        long double k4[4] = {a, bb, cc, det};
+        for (int q = 0; q < 4; q++) split_ld(k4[q], &L->lm[(size_t)q * nc + c], &L->les[(size_t)q * nc + c]);
+        L->lrv[c] = recip64(L->lm[(size_t)3 * nc + c]);
         for (int j = 0; j < np; j++) {
+            L->ldx[(size_t)j * nc + c] = dx[j];
+            L->ldy[(size_t)j * nc + c] = dy[j];
             L->wx[(size_t)j * nc + c] = (double)((cc * dx[j] - bb * dy[j]) / det);
             L->wy[(size_t)j * nc + c] = (double)((-bb * dx[j] + a * dy[j]) / det);
         }

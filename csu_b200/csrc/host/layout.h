@@ -30,6 +30,11 @@ typedef struct csu_layout {
     int* nei;      /* [4][nc] neighbour (ELEMENT.neiL order): cell id, or nc + boundary face id       */
     double* wx;    /* [4][nc] least-squares weights: dUx = sum wx (u_nei - u_cell)                     */
     double* wy;
+    double* ldx;   /* [4][nc] neighbour centre minus centroid, x and y (solverCalcGrad3 x[jj] - x[0])   */
+    double* ldy;
+    unsigned long long* lm;  /* [4][nc] x87 significands of a, b, c, a*c - b*b (long double, solver.c:1058-1073) */
+    int* les;      /* [4][nc] exponent << 1 | sign of the same                                          */
+    unsigned long long* lrv; /* [nc] invariant-divisor reciprocal of the determinant's significand       */
     double* ex;    /* [4][nc] edge midpoint minus centroid, edges in node order (limiter, inter)        */
     double* ey;
     int* fslot;    /* [4][nc] +-(flux index + 1): interior faces (ELEMENT.f order) then boundary faces  */

@@ -180,6 +180,23 @@ int csu_tube_run(csu_ctx* ctx, double tmax, int* steps, double* t_final);
 #define CSU_DUMP_BLOCKS 10
 int csu_dump(csu_ctx* ctx, int what, double* out);
 
+/* Run the engine's work on a caller-provided cudaStream_t (NULL: the context's own stream). */
+int csu_set_stream(csu_ctx* ctx, void* stream);
+
+/* Kernel kinds of csu_time_kernels. */
+#define CSU_K_PRIM 0     /* primitives + clamps (solverCalcPrimitive)                    */
+#define CSU_K_GRAD 1     /* least-squares gradient + limiter (solverUpdateGrad, inter)    */
+#define CSU_K_FLUX 2     /* interior and boundary face fluxes (inter, boundary)           */
+#define CSU_K_RK 3       /* residual gather + RK stage (solverRK)                         */
+#define CSU_K_IMPL 4     /* residual gather + implicit diagonal + DPLUR blocks            */
+#define CSU_K_SWEEP 5    /* one DPLUR Jacobi sweep                                        */
+#define CSU_K_FINALIZE 6 /* norms, force coefficients, step size                          */
+#define CSU_K_RESID 7    /* residual gather only                                          */
+#define CSU_K_COUNT 8
+/* Runs `iters` iterations with a CUDA event after every kernel and returns, per kind, the summed device
+ * time in ms and the launch count (the iterations advance the state like csu_iterate). */
+int csu_time_kernels(csu_ctx* ctx, int iters, double* ms, int* count);
+
 /* Counters of the engine: kernels launched since creation, device bytes held. */
 int csu_stats(csu_ctx* ctx, long long* kernel_launches, long long* device_bytes);
 
