@@ -134,11 +134,17 @@ static void plan(csu_ctx* x, Arena& a)
     m.fds = carve<double>(a, nf);
     m.r0 = carve<double2>(a, nf);
     m.r1 = carve<double2>(a, nf);
+    m.fd = carve<double2>(a, nf);
+    m.fL = carve<double>(a, nf);
     m.bown = carve<int>(a, nb);
     m.bflag = carve<int>(a, nb);
     m.bold = carve<int>(a, nb);
     m.bn = carve<double2>(a, nb);
     m.bds = carve<double>(a, nb);
+    m.bd = carve<double2>(a, nb);
+    m.bL = carve<double>(a, nb);
+    m.bun = carve<double2>(a, nb);
+    m.bds2 = carve<double>(a, nb);
     x->d_wall_rank = carve<int>(a, nb);
 
     s.U4 = carve<double4>(a, nc);
@@ -149,6 +155,10 @@ static void plan(csu_ctx* x, Arena& a)
     s.G4x = carve<double4>(a, nc);
     s.G4y = carve<double4>(a, nc);
     s.PH4 = carve<double4>(a, nc);
+    int visc = x->cfg.laminar || x->cfg.sa || x->cfg.sst;
+    s.GTx = carve<double>(a, visc ? nc : 0);
+    s.GTy = carve<double>(a, visc ? nc : 0);
+    s.FV = carve<double4>(a, visc ? (size_t)nf + nb : 0);
     s.Gxx = carve<double>(a, (size_t)nx * nc);
     s.Gxy = carve<double>(a, (size_t)nx * nc);
     s.PHx = carve<double>(a, (size_t)nx * nc);
@@ -181,14 +191,19 @@ static int upload_mesh(csu_ctx* x)
         return cudaMemcpy(const_cast<void*>(dst), src, bytes, cudaMemcpyHostToDevice);
     };
     std::vector<int2> fe(nf);
-    std::vector<double2> fn(nf), r0(nf), r1(nf), bn(nb);
+    std::vector<double2> fn(nf), r0(nf), r1(nf), bn(nb), fd(nf), bd(nb), bun(nb);
     for (int f = 0; f < nf; f++) {
         fe[f] = make_int2(L.fe0[f], L.fe1[f]);
+        fd[f] = make_double2(L.fdx[f], L.fdy[f]);
         fn[f] = make_double2(L.fdsx[f], L.fdsy[f]);
         r0[f] = make_double2(L.r0x[f], L.r0y[f]);
         r1[f] = make_double2(L.r1x[f], L.r1y[f]);
     }
-    for (int b = 0; b < nb; b++) bn[b] = make_double2(L.bdsx[b], L.bdsy[b]);
+    for (int b = 0; b < nb; b++) {
+        bn[b] = make_double2(L.bdsx[b], L.bdsy[b]);
+        bd[b] = make_double2(L.bdx[b], L.bdy[b]);
+        bun[b] = make_double2(L.bunx[b], L.buny[b]);
+    }
     // walls in reference order (solverCalcCoeff3 sums over wall markers, marker-major)
     std::vector<int> rank(nb > 0 ? nb : 1, -1);
     {
@@ -225,11 +240,17 @@ static int upload_mesh(csu_ctx* x)
     CK(up(m.fds, L.fds, sizeof(double) * nf));
     CK(up(m.r0, r0.data(), sizeof(double2) * nf));
     CK(up(m.r1, r1.data(), sizeof(double2) * nf));
+    CK(up(m.fd, fd.data(), sizeof(double2) * nf));
+    CK(up(m.fL, L.fdist, sizeof(double) * nf));
     CK(up(m.bown, L.bown, sizeof(int) * nb));
     CK(up(m.bflag, L.bflag, sizeof(int) * nb));
     CK(up(m.bold, L.bold, sizeof(int) * nb));
     CK(up(m.bn, bn.data(), sizeof(double2) * nb));
     CK(up(m.bds, L.bds, sizeof(double) * nb));
+    CK(up(m.bd, bd.data(), sizeof(double2) * nb));
+    CK(up(m.bL, L.bL, sizeof(double) * nb));
+    CK(up(m.bun, bun.data(), sizeof(double2) * nb));
+    CK(up(m.bds2, L.bds2, sizeof(double) * nb));
     CK(up(x->d_wall_rank, rank.data(), sizeof(int) * nb));
     return CSU_OK;
 }
@@ -288,6 +309,7 @@ static void fill_params(csu_ctx* x)
     // exact x87 gradients unless CSU_LSQ_FAST=1 (FP64 weights: faster, last-bit differences)
     const char* fast = getenv("CSU_LSQ_FAST");
     p.lsq_exact = (fast && fast[0] == '1') ? 0 : 1;
+    p.visc = (c.laminar || c.sa || c.sst) ? 1 : 0;
     p.conv_tol = 0;
 }
 
@@ -322,8 +344,8 @@ extern "C" int csu_create(const csu_mesh_desc* md, const csu_config* cfg, csu_ct
         csu_set_error("csu_create: nvar %d does not match the turbulence model", cfg->nvar);
         return CSU_ERR_INPUT;
     }
-    if (model != 0 || cfg->laminar) {
-        csu_set_error("csu_create: viscous and turbulent models are not available in this engine build");
+    if (model != 0) {
+        csu_set_error("csu_create: turbulence models are not available in this engine build");
         return CSU_ERR_UNSUPPORTED;
     }
     if (cfg->time_scheme == CSU_TS_LUSGS) {
@@ -516,7 +538,7 @@ static void launch_iteration(csu_ctx* x)
     if (c.time_scheme == CSU_TS_RK) {
         for (int sgi = 0; sgi < c.stages; sgi++) {
             bool last = sgi == c.stages - 1;
-            if (c.order == 2) launch_grad<MODEL>(x, false);
+            if (c.order == 2 || x->prm.visc) launch_grad<MODEL>(x, false);
             launch_flux<MODEL>(x, last ? 1 : 0);
             if (last) k_rk<MODEL, true><<<x->gb_c, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st, x->rk[sgi]);
             else k_rk<MODEL, false><<<x->gb_c, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st, x->rk[sgi]);
@@ -525,7 +547,7 @@ static void launch_iteration(csu_ctx* x)
         }
         launch_finalize<MODEL>(x, 0);
     } else {
-        if (c.order == 2) launch_grad<MODEL>(x, false);
+        if (c.order == 2 || x->prm.visc) launch_grad<MODEL>(x, false);
         launch_flux<MODEL>(x, 1);
         k_impl<MODEL, true><<<x->gb_c, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st);
         x->launches++;

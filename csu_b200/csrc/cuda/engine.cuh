@@ -4,6 +4,7 @@
 #include <stdint.h>
 #include "physics.cuh"
 #include "ext80.cuh"
+#include "viscous.cuh"
 
 namespace csu {
 
@@ -23,6 +24,7 @@ struct Prm {
     int nc, nf, nb;
     int order, scheme, laminar, sa, sst, axi, turb1order, limiter_type, stages, dt_local_n, tube, n_linear;
     int lsq_exact;      // gradients with the reference's x87 rounding (1) or precomputed FP64 weights (0)
+    int visc;           // laminar, SA or SST: temperature gradient and viscous fluxes
     double lim_k, vol_max, e_fix, r_lim, p_out, t_wall, pr, pr_t, w_imp, cfl, sigma, mach_inf, sref;
     double pin[7];
     double pref20[6];   // limiterUpdate type 0 reference squares (limiter.c:49-59)
@@ -78,17 +80,25 @@ struct Mesh {
     const double* fds;
     const double2* r0;
     const double2* r1;
+    const double2* fd;              // centroid of e1 minus centroid of e0
+    const double* fL;               // |fd|
     const int* bown;
     const int* bflag;
     const int* bold;
     const double2* bn;
     const double* bds;
+    const double2* bd;              // boundary edge midpoint minus owner centroid
+    const double* bL;               // |bd|
+    const double2* bun;             // unit normal of meshCalcDS2 (unscaled)
+    const double* bds2;             // |dS| of meshCalcDS2 (axisymmetric: times the mean y)
 };
 
 struct State {
     double4* U4;  double* Ux;                 // conserved state (after the write-back clamps)
     double4* W4;  double* WT;  double* Wx;    // primitives of the cells
     double4* G4x; double4* G4y; double4* PH4; // gradients and limiter (r u v p)
+    double* GTx;  double* GTy;                // temperature gradient (solverGrad_T, viscous models)
+    double4* FV;                              // viscous face fluxes (x, y momentum, energy)
     double* Gxx;  double* Gxy;  double* PHx;  // same for the scalars, [k][cell]
     double4* F4;  double* Fx;                 // face fluxes * |dS|: nf interior then nb boundary
     double4* R4;  double* Rx;                 // residual

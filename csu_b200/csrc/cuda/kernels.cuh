@@ -68,7 +68,9 @@ __global__ void __launch_bounds__(BLOCK) k_grad(const __grid_constant__ Prm p, c
     double P0[NP];
     loadP<MODEL>(s, nc, c, P0);
     double gx[NV], gy[NV], qmin[NV], qmax[NV];
-    X80 XA[NV], XB[NV];
+    X80 XA[NV], XB[NV], TA = x80_zero(0), TB = x80_zero(0);
+    double gtx = 0.0, gty = 0.0;
+    const bool visc = p.visc != 0;
 #pragma unroll
     for (int kk = 0; kk < NV; kk++) {
         gx[kk] = 0.0;
@@ -100,6 +102,11 @@ __global__ void __launch_bounds__(BLOCK) k_grad(const __grid_constant__ Prm p, c
             if (exact) {
                 // solverCalcGrad3 (solver.c:1063-1070): double products summed in long double
                 double dxj = m.ldx[(size_t)j * nc + c], dyj = m.ldy[(size_t)j * nc + c];
+                if (visc) {
+                    double dT = Pn[4] - P0[4];
+                    TA = x80_add(TA, x80_from_double(dxj * dT));
+                    TB = x80_add(TB, x80_from_double(dyj * dT));
+                }
 #pragma unroll
                 for (int kk = 0; kk < NV; kk++) {
                     double du = Pn[slot2p(kk)] - P0[slot2p(kk)];
@@ -110,6 +117,11 @@ __global__ void __launch_bounds__(BLOCK) k_grad(const __grid_constant__ Prm p, c
                 }
             } else {
                 double wxj = m.wx[(size_t)j * nc + c], wyj = m.wy[(size_t)j * nc + c];
+                if (visc) {
+                    double dT = Pn[4] - P0[4];
+                    gtx += wxj * dT;
+                    gty += wyj * dT;
+                }
 #pragma unroll
                 for (int kk = 0; kk < NV; kk++) {
                     double du = Pn[slot2p(kk)] - P0[slot2p(kk)];
@@ -139,6 +151,17 @@ __global__ void __launch_bounds__(BLOCK) k_grad(const __grid_constant__ Prm p, c
             gx[kk] = x80_to_double(x80_div_pre(nx, K[3], rv));
             gy[kk] = x80_to_double(x80_div_pre(ny, K[3], rv));
         }
+        if (visc) {
+            // solverGrad_T (solver.c:477-490): the same least squares on T
+            X80 nx = x80_add(x80_mul(K[2], TA), x80_neg(x80_mul(K[1], TB)));
+            X80 ny = x80_add(x80_mul(x80_neg(K[1]), TA), x80_mul(K[0], TB));
+            gtx = x80_to_double(x80_div_pre(nx, K[3], rv));
+            gty = x80_to_double(x80_div_pre(ny, K[3], rv));
+        }
+    }
+    if (visc) {
+        s.GTx[c] = gtx;
+        s.GTy[c] = gty;
     }
     double phi[NV];
 #pragma unroll
@@ -236,6 +259,15 @@ __global__ void __launch_bounds__(BLOCK) k_flux(const __grid_constant__ Prm p, c
                 PR[kk] = B[slot2p(kk)];
             }
         }
+        if (p.laminar == 1) {
+            double4 a = s.G4x[e.x], b = s.G4y[e.x], cc = s.G4x[e.y], d = s.G4y[e.y];
+            double g0x[3] = {a.y, a.z, s.GTx[e.x]}, g0y[3] = {b.y, b.z, s.GTy[e.x]};
+            double g1x[3] = {cc.y, cc.z, s.GTx[e.y]}, g1y[3] = {d.y, d.z, s.GTy[e.y]};
+            double2 dd = m.fd[f];
+            double fv[3];
+            laminar_face(p.gas, p.pr, g0x, g0y, g1x, g1y, A, B, dd.x, dd.y, m.fL[f], dSx, dSy, fv);
+            s.FV[f] = make_double4(fv[0], fv[1], fv[2], 0.0);
+        }
         rotation(PL, dSx, dSy, dS);
         rotation(PR, dSx, dSy, dS);
         double fl[NV];
@@ -261,6 +293,23 @@ __global__ void __launch_bounds__(BLOCK) k_flux(const __grid_constant__ Prm p, c
                           : make_double4(0.0, 0.0, 0.0, 0.0);
 #pragma unroll
         for (int kk = 4; kk < NV; kk++) s.Fx[(size_t)(kk - 4) * (m.nf + m.nb) + fi] = dS > 0 ? fl[kk] * sc : 0.0;
+        double gvx[3], gvy[3];
+        double2 bdv = make_double2(0.0, 0.0);
+        double bLv = 0.0;
+        if (p.visc) {
+            double4 a = s.G4x[c], bb = s.G4y[c];
+            gvx[0] = a.y; gvx[1] = a.z; gvx[2] = s.GTx[c];
+            gvy[0] = bb.y; gvy[1] = bb.z; gvy[2] = s.GTy[c];
+            bdv = m.bd[b];
+            bLv = m.bL[b];
+        }
+        if (p.laminar == 1) {
+            double2 un = m.bun[b];
+            double fv[3];
+            laminar_boundary(p.gas, p.pr, p.t_wall, p.pin, flag, gvx, gvy, E0, dSx, dSy, bdv.x, bdv.y, bLv, un.x,
+                             un.y, m.bds2[b], fv);
+            s.FV[fi] = make_double4(fv[0], fv[1], fv[2], 0.0);
+        }
         if (coef && (flag == 3 || flag == 4)) {
             double G[NP];
             ghost_state<MODEL>(p, flag, dSx, dSy, dS, E0, m.wall_d ? m.wall_d[c] : 0.0, G);
@@ -268,8 +317,10 @@ __global__ void __launch_bounds__(BLOCK) k_flux(const __grid_constant__ Prm p, c
             int r = wall_rank[b];
             s.bcoef[(size_t)r * 4 + 0] = cp * dSx;
             s.bcoef[(size_t)r * 4 + 1] = cp * dSy;
-            s.bcoef[(size_t)r * 4 + 2] = 0.0;
-            s.bcoef[(size_t)r * 4 + 3] = 0.0;
+            double fx = 0.0, fy = 0.0;
+            if (p.visc) friction_wall(gvx, gvy, E0, dSx, dSy, bdv.x, bdv.y, bLv, &fx, &fy);
+            s.bcoef[(size_t)r * 4 + 2] = p.visc ? fx / p.q_inf : 0.0;
+            s.bcoef[(size_t)r * 4 + 3] = p.visc ? fy / p.q_inf : 0.0;
         }
     }
 }
@@ -308,6 +359,27 @@ __device__ __forceinline__ void gather_residual(const Prm& p, const Mesh& m, con
         double dS = m.dslat[c];
         R[2] -= P[3] * dS;
         if constexpr (MODEL == 2) R[2] -= (2. / 3.) * P[0] * P[5] * dS;
+    }
+    if (p.laminar == 1) {
+        // laminarInter gather then laminarBoundary (laminar.c:77-125)
+        const int ni = m.nint[c];
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            if (j < ns) {
+                int sf = m.fslot[(size_t)j * nc + c];
+                int fi = sf > 0 ? sf - 1 : -sf - 1;
+                double4 V = s.FV[fi];
+                if (j >= ni || sf > 0) {
+                    R[1] -= V.x;
+                    R[2] -= V.y;
+                    R[3] -= V.z;
+                } else {
+                    R[1] += V.x;
+                    R[2] += V.y;
+                    R[3] += V.z;
+                }
+            }
+        }
     }
 }
 
@@ -429,7 +501,7 @@ __global__ void __launch_bounds__(BLOCK) k_impl(const __grid_constant__ Prm p, c
         gather_residual<MODEL>(p, m, s, c, P, R);
         storeR<MODEL>(s, nc, c, R);
         const int ni = m.nint[c], ns = m.nslot[c];
-        double Lc = 0;
+        double Lc = 0, Lv = 0;
         for (int j = 0; j < ni; j++) {
             int sf = m.fslot[(size_t)j * nc + c];
             int f = sf > 0 ? sf - 1 : -sf - 1;
@@ -444,8 +516,13 @@ __global__ void __launch_bounds__(BLOCK) k_impl(const __grid_constant__ Prm p, c
             double cc = T2c(p.gas, T);
             double nx = dSv.x / dS, ny = dSv.y / dS;
             Lc += (fabs(nx * u + ny * v) + cc) * dS;
+            if (p.laminar) {
+                double r = (w0.x + w1.x) * 0.5;
+                Lv += visc_radius(p.gas, p.pr, r, T) * dS * dS;
+            }
         }
         double D = 0.5 * p.w_imp * Lc;
+        if (p.visc) D += Lv / m.omega[c];
         for (int j = ni; j < ns; j++) {
             int b = m.fslot[(size_t)j * nc + c] - 1 - m.nf;
             double2 dSv = m.bn[b];
@@ -462,6 +539,10 @@ __global__ void __launch_bounds__(BLOCK) k_impl(const __grid_constant__ Prm p, c
             double Lb = (fabs(nx * P[1] + ny * P[2]) + cc) * dS;
             Lc += Lb;
             D += 0.5 * p.w_imp * Lb;
+            if (p.visc) {
+                double Lvb = visc_radius(p.gas, p.pr, P[0], P[4]) * dS * dS;
+                D += Lvb / m.omega[c];
+            }
         }
         double om = m.omega[c];
         double l = om / Lc;
@@ -507,6 +588,11 @@ __global__ void __launch_bounds__(BLOCK) k_impl(const __grid_constant__ Prm p, c
                 }
                 double cc = T2c(p.gas, Pn[4]);
                 double ra = p.w_imp * (fabs(nx * Pn[1] + ny * Pn[2]) + cc) * dS;
+                if (p.laminar) {
+                    double r = (P[0] + Pn[0]) * 0.5;
+                    double T = (P[4] + Pn[4]) * 0.5;
+                    ra += visc_radius(p.gas, p.pr, r, T) * dS / m.fL[f];
+                }
 #pragma unroll
                 for (int nn = 0; nn < NV; nn++) A[(size_t)(nn * NV + nn) * nc] -= 0.5 * ra;
             }
@@ -639,7 +725,9 @@ __global__ void __launch_bounds__(BLOCK) k_finalize(const __grid_constant__ Prm 
             sc->res[k] = sqrt(v[k] / m.nc);
             if (!isfinite(sc->res[k])) bad = true;
         }
-        double cxp = v[NV] / p.sref, cyp = v[NV + 1] / p.sref, cxv = v[NV + 2] / p.sref, cyv = v[NV + 3] / p.sref;
+        // Cx_v -= fx/q per wall face (solver.c:1376-1380): the negated sum
+        double cxp = v[NV] / p.sref, cyp = v[NV + 1] / p.sref;
+        double cxv = (0.0 - v[NV + 2]) / p.sref, cyv = (0.0 - v[NV + 3]) / p.sref;
         if (p.axi) {
             cxp *= 2 * M_PI;
             cxv *= 2 * M_PI;

@@ -114,7 +114,8 @@ void csu_layout_free(csu_layout* L)
                     L->bface_old2new, L->npts, L->nint, L->nslot, L->nei, L->wx, L->wy, L->ex, L->ey,
                     L->fslot, L->omega, L->sxh, L->syh, L->xc, L->yc, L->wall_d, L->dslat, L->fe0, L->fe1,
                     L->fdsx, L->fdsy, L->fds, L->r0x, L->r0y, L->r1x, L->r1y, L->fdist, L->bown, L->bflag,
-                    L->bold, L->bdsx, L->bdsy, L->bds, L->bmx, L->bmy, L->ldx, L->ldy, L->lm, L->les, L->lrv};
+                    L->bold, L->bdsx, L->bdsy, L->bds, L->bmx, L->bmy, L->ldx, L->ldy, L->lm, L->les, L->lrv,
+                    L->fdx, L->fdy, L->bdx, L->bdy, L->bL, L->bunx, L->buny, L->bds2};
     for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); i++) free(ptrs[i]);
     memset(L, 0, sizeof(*L));
 }
@@ -141,6 +142,8 @@ int csu_layout_build(const csu_mesh_desc* m, int axi, csu_layout* L)
     ALLOC(L->r0x, nf); ALLOC(L->r0y, nf); ALLOC(L->r1x, nf); ALLOC(L->r1y, nf); ALLOC(L->fdist, nf);
     ALLOC(L->bown, nb); ALLOC(L->bflag, nb); ALLOC(L->bold, nb); ALLOC(L->bdsx, nb); ALLOC(L->bdsy, nb);
     ALLOC(L->bds, nb); ALLOC(L->bmx, nb); ALLOC(L->bmy, nb);
+    ALLOC(L->fdx, nf); ALLOC(L->fdy, nf); ALLOC(L->bdx, nb); ALLOC(L->bdy, nb); ALLOC(L->bL, nb);
+    ALLOC(L->bunx, nb); ALLOC(L->buny, nb); ALLOC(L->bds2, nb);
 #undef ALLOC
     if (!L->bmy || !L->fslot || !L->fdist) {
         csu_layout_free(L);
@@ -219,7 +222,9 @@ int csu_layout_build(const csu_mesh_desc* m, int axi, csu_layout* L)
         L->r0y[f] = ym - cy[e0];
         L->r1x[f] = xm - cx[e1];
         L->r1y[f] = ym - cy[e1];
-        L->fdist[f] = sqrt((cx[e1] - cx[e0]) * (cx[e1] - cx[e0]) + (cy[e1] - cy[e0]) * (cy[e1] - cy[e0]));
+        L->fdx[f] = cx[e1] - cx[e0];
+        L->fdy[f] = cy[e1] - cy[e0];
+        L->fdist[f] = sqrt(L->fdx[f] * L->fdx[f] + L->fdy[f] * L->fdy[f]);
     }
     /* boundary faces */
     for (int b = 0; b < nb; b++) {
@@ -236,6 +241,20 @@ int csu_layout_build(const csu_mesh_desc* m, int axi, csu_layout* L)
         /* elementCenter of the two-node boundary element */
         L->bmx[b] = (m->xy[2 * p0] + m->xy[2 * p1]) / 2;
         L->bmy[b] = (m->xy[2 * p0 + 1] + m->xy[2 * p1 + 1]) / 2;
+        {
+            int ow = m->bface[3 * o + 2];
+            double ox = 0.0, oy = 0.0;
+            center(m, ow, &ox, &oy);
+            double x1 = (m->xy[2 * p0] + m->xy[2 * p1]) * 0.5, y1 = (m->xy[2 * p0 + 1] + m->xy[2 * p1 + 1]) * 0.5;
+            L->bdx[b] = x1 - ox;
+            L->bdy[b] = y1 - oy;
+            L->bL[b] = sqrt(L->bdx[b] * L->bdx[b] + L->bdy[b] * L->bdy[b]);
+            double ux = m->xy[2 * p1 + 1] - m->xy[2 * p0 + 1], uy = -(m->xy[2 * p1] - m->xy[2 * p0]);
+            double s2 = sqrt(ux * ux + uy * uy);
+            L->bunx[b] = ux / s2;
+            L->buny[b] = uy / s2;
+            L->bds2[b] = axi == 1 ? s2 * (m->xy[2 * p0 + 1] + m->xy[2 * p1 + 1]) * 0.5 : s2;
+        }
     }
     free(oflag);
 

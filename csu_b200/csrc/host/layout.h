@@ -57,6 +57,8 @@ typedef struct csu_layout {
     double* r1x;
     double* r1y;
     double* fdist; /* centroid distance |x_e1 - x_e0| (viscous terms)                                 */
+    double* fdx;   /* x_e1 - x_e0, y_e1 - y_e0 (laminar.c:44-45)                                        */
+    double* fdy;
 
     /* per renumbered boundary face */
     int* bown;
@@ -67,6 +69,12 @@ typedef struct csu_layout {
     double* bds;
     double* bmx;   /* edge midpoint (ghost centre)                                                    */
     double* bmy;
+    double* bdx;   /* edge midpoint minus owner centroid, and its length (laminar.c:184-191)            */
+    double* bdy;
+    double* bL;
+    double* bunx;  /* meshCalcDS2 unit normal and length (mesh.c:742-764)                               */
+    double* buny;
+    double* bds2;
 
     double vol_max;/* max omega (limiterUpdate type 0, limiter.c:44-48)                               */
     int max_npts;

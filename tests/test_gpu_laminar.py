@@ -1,0 +1,58 @@
+"""Laminar Navier-Stokes path (laminar.c) vs the reference on its laminar example cases (flat plate,
+NACA 0012 at M 0.1). The reference leaves the energy term of adiabatic-wall viscous fluxes unset
+(laminar.c:104-115, 230-268: an uninitialised local); those entries are excluded and reported."""
+import numpy as np
+import pytest
+
+import casekit
+
+pytestmark = pytest.mark.gpu
+LAMINAR = ["caseBL", "caseNACA0012"]
+
+
+def _setup(name, kv=None):
+    import csu_b200
+    from oracle.refharness import Ref, available
+    if not available():
+        pytest.skip("reference build oracle/_ref missing")
+    kv = dict(casekit.GOLDEN_OVERRIDES.get(name, {}), **(kv or {}))
+    wd = casekit.materialize(name, kv)
+    case = csu_b200.Case.load(wd)
+    return csu_b200.Engine(case), case, Ref(wd)
+
+
+def _adiabatic_wall_cells(case):
+    flags = np.repeat(case.marker_flag, case.marker_nbf)
+    return np.unique(case.bface[flags == 3, 2])
+
+
+@pytest.mark.parametrize("name", LAMINAR)
+def test_laminar_residual(native, name):
+    eng, case, ref = _setup(name)
+    ref.iterate(3)
+    U = ref.get_U()
+    eng.set_state(U)
+    R_ref = ref.calc_R()
+    R = eng.residual()
+    mask = np.ones_like(R, dtype=bool)
+    mask[3, _adiabatic_wall_cells(case)] = False
+    diff = np.count_nonzero(R[mask] != R_ref[mask])
+    print("%s: %d/%d differ outside adiabatic-wall energy entries" % (name, diff, mask.sum()))
+    assert diff == 0
+    G = eng.dump("GRAD")
+    assert np.array_equal(G[:, :3], ref.grad()[:, :3])
+
+
+@pytest.mark.parametrize("name,scheme", [("caseBL", "RK"), ("caseNACA0012", "DPLUR")])
+def test_laminar_history(native, name, scheme):
+    kv = {"timeScheme": scheme}
+    if scheme == "DPLUR":
+        kv.update({"Nlinear": "4", "CFL": "2.0"})
+    eng, case, ref = _setup(name, kv)
+    n = 10
+    h_ref = ref.iterate(n)
+    h = eng.iterate(n)
+    nv = case.nvar
+    rel = np.max(np.abs(h[:, :nv] - h_ref[:, :nv]) / (np.abs(h_ref[:, :nv]) + 1e-300))
+    print("%s %s: history max rel %.3e" % (name, scheme, rel))
+    assert rel < 1e-9

@@ -1,0 +1,157 @@
+"""Host C front end vs the reference (CPU only): SU2 reading, face hashing order, neighbour order,
+boundary matching/orientation, wall distance, initial state, keyword parsing, error statuses."""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+import casekit
+
+
+def _ref(wd):
+    from oracle.refharness import Ref, available
+    if not available():
+        pytest.skip("reference build oracle/_ref missing (needs the reference tree)")
+    return Ref(wd)
+
+
+@pytest.mark.parametrize("name", casekit.CASES)
+def test_mesh_integer_exact(native, name):
+    import csu_b200
+    wd = casekit.materialize(name, casekit.GOLDEN_OVERRIDES.get(name, {}))
+    case = csu_b200.Case.load(wd)
+    ref = _ref(wd)
+    m = ref.mesh()
+    assert (case.n_cells, case.n_faces, case.n_bfaces) == (ref.nc, ref.nf, ref.nb)
+    assert np.array_equal(case.con.ravel(), m["con"])
+    assert np.array_equal(case.cell_nodes.ravel(), m["nodes"])
+    assert np.array_equal(case.cell_faces.ravel(), m["f"])
+    assert np.array_equal(case.cell_nint, m["nint"])
+    assert np.array_equal(case.cell_nei.ravel(), m["nei"])
+    assert np.array_equal(case.bface.ravel(), m["bface"])
+    assert np.array_equal(case.marker_flag, m["marker_flag"])
+    assert np.array_equal(case.xy.ravel(), m["xy"])
+    if "wall_dist" in m:
+        assert np.array_equal(case.wall_dist, m["wall_dist"])
+    assert np.array_equal(case.initial_state(), ref.get_U())
+
+
+def test_generated_meshes_integer_exact(native):
+    import csu_b200
+    from csu_b200 import meshgen
+    for su2, inp in (meshgen.ramp(ni=40, nj=20), meshgen.sod_tube(ni=50)):
+        wd = casekit.write_case(inp, su2, "gen")
+        case = csu_b200.Case.load(wd)
+        m = _ref(wd).mesh()
+        assert np.array_equal(case.con.ravel(), m["con"])
+        assert np.array_equal(case.cell_nei.ravel(), m["nei"])
+        assert np.array_equal(case.bface.ravel(), m["bface"])
+
+
+def _ref_input(path):
+    """The reference's own keyword parser, inputInit (input.c:7-95), through the built reference."""
+    from oracle.refharness import LIB, available
+    if not available():
+        pytest.skip("reference build oracle/_ref missing")
+
+    class INPUT(C.Structure):
+        _fields_ = [("N", C.c_int), ("Nmax", C.c_int), ("name", C.POINTER(C.c_char_p)),
+                    ("value", C.POINTER(C.c_char_p))]
+
+    L = C.CDLL(LIB)
+    L.inputInit.restype = C.POINTER(INPUT)
+    L.inputInit.argtypes = [C.c_char_p, C.c_int]
+    inp = L.inputInit(path.encode(), 50).contents
+    return [(inp.name[i].decode(), inp.value[i].decode()) for i in range(inp.N)]
+
+
+KEYWORD_TEXTS = [
+    "a, 1\nb, 2\n",
+    "a , 1 \r\nb,2\r\n c d , 3 4\n",
+    "a, 1 # comment\nb, 2\nc, 3\n",
+    "#header\na, 1\n",
+    "name_only\nx, 5\n\n\n",
+    "a, 1\na, 2\n",
+    "a, 1, 2\n",
+    "a, 1\nb, 2",
+]
+
+
+@pytest.mark.parametrize("text", KEYWORD_TEXTS)
+def test_keyword_parser_matches_reference(native, text, tmp_path):
+    import csu_b200
+    p = str(tmp_path / "input.dat")
+    with open(p, "w", newline="") as f:
+        f.write(text)
+    expect = _ref_input(p)
+    # through the engine's parser: build a minimal case around the keyword text and read every key back
+    mesh = casekit.read_mesh("caseWedgeQuad")
+    base = casekit.read_input("caseWedgeQuad")
+    case = csu_b200.Case.from_text(base, mesh)
+    # direct check of the parser via a case whose input is text + the required keys
+    full = text + ("\n" if not text.endswith("\n") else "") + base
+    for k, v in expect:
+        if not k:
+            continue
+        try:
+            case2 = csu_b200.Case.from_text(full, mesh)
+        except csu_b200.CsuError:
+            pytest.skip("text changes required keys")
+        got = [None]
+        try:
+            got[0] = case2.get_double(k)
+        except csu_b200.CsuError:
+            got[0] = None
+        # reference lookups return the last entry of a name: compare through strtod of the value
+        last = [vv for kk, vv in expect if kk == k][-1]
+        import math
+        want = float(last) if _isfloat(last) else 0.0
+        if got[0] is not None and _isfloat(last):
+            assert got[0] == want or (math.isnan(got[0]) and math.isnan(want))
+    assert case is not None
+
+
+def _isfloat(s):
+    try:
+        float(s)
+        return True
+    except ValueError:
+        return False
+
+
+def test_errors_are_statuses(native):
+    import csu_b200
+    mesh = casekit.read_mesh("caseWedgeQuad")
+    base = casekit.read_input("caseWedgeQuad")
+    with pytest.raises(csu_b200.CsuError) as e:
+        csu_b200.Case.from_text(base.replace("flux, ROE", "flux, NOPE"), mesh)
+    assert e.value.status == 1 and "flux choice" in str(e.value)
+    with pytest.raises(csu_b200.CsuError) as e:
+        csu_b200.Case.from_text(base.replace("CFL", "XFL"), mesh)
+    assert e.value.status == 1 and "CFL" in str(e.value)
+    with pytest.raises(csu_b200.CsuError) as e:
+        csu_b200.Case.from_text(base.replace("BC:wall1, wall", "BC:wall1, hole"), mesh)
+    assert e.value.status == 1
+    with pytest.raises(csu_b200.CsuError) as e:
+        csu_b200.Case.from_text(base, mesh[: len(mesh) // 2])
+    assert e.value.status == 1
+    with pytest.raises(csu_b200.CsuError) as e:
+        csu_b200.Case.from_text(base, mesh.replace("\n5 ", "\n7 ", 1))
+    assert e.value.status == 1 and "type" in str(e.value)
+    with pytest.raises(csu_b200.CsuError) as e:
+        csu_b200.Case.load("/nonexistent_dir_xyz/")
+    assert e.value.status == 2
+
+
+def test_restart_roundtrip(native):
+    import csu_b200
+    mesh = casekit.read_mesh("caseWedgeQuad")
+    base = casekit.read_input("caseWedgeQuad")
+    case = csu_b200.Case.from_text(base, mesh)
+    U = case.initial_state() * (1 + 0.01 * np.arange(case.n_cells)[None, :] / case.n_cells)
+    lines = ["1,", "0, %d, %d," % (case.n_cells, case.nvar)]
+    lines += ["".join("%.10e, " % U[k, i] for k in range(case.nvar)) for i in range(case.n_cells)]
+    restart = "\n".join(lines) + "\n"
+    case2 = csu_b200.Case.from_text(casekit.override(base, {"restart": "1"}), mesh, restart)
+    assert np.allclose(case2.initial_state(), U, rtol=1e-10)
