@@ -103,7 +103,10 @@ def test_history_parity(native, name):
     h_ref = ref.iterate(n)
     h = eng.iterate(n)
     assert h.shape == h_ref.shape
-    assert np.array_equal(h[:, :case.nvar], h_ref[:, :case.nvar])
+    # the state is the reference's bit for bit; the RMS norms differ in the last bits only because the
+    # device sums the squares in a different order than the reference's serial loop
+    assert np.array_equal(eng.get_state(), ref.get_U())
+    assert _rel(h[:, :case.nvar], h_ref[:, :case.nvar]) < 1e-13
     nv = case.nvar
     assert _rel(h[:, :nv], h_ref[:, :nv]) < RTOL_HIST
     cs = np.abs(h_ref[:, nv:]).max() + 1e-300
