@@ -92,6 +92,7 @@ def lib():
         L.csu_stats.argtypes = [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
         L.csu_set_stream.argtypes = [vp, vp]
         L.csu_time_kernels.argtypes = [vp, C.c_int, dp, ip]
+        L.csu_residual_norms_noalloc.argtypes = [vp, C.c_int, C.c_int, vp, vp]
         _lib = L
     return _lib
 

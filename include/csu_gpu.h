@@ -197,6 +197,17 @@ int csu_set_stream(csu_ctx* ctx, void* stream);
  * time in ms and the launch count (the iterations advance the state like csu_iterate). */
 int csu_time_kernels(csu_ctx* ctx, int iters, double* ms, int* count);
 
+/* Residual RMS norms res[k] = sqrt(sum_i R[k][i]^2 / ncells) -- the quantity of solverCalcRes -- from a
+ * residual the caller holds in device memory ([var][cell], nvar <= 6), written to the caller's device array
+ * res (nvar doubles), asynchronously on `stream` (a cudaStream_t, NULL for the default stream). No
+ * counterpart in the reference: this entry allocates nothing, for callers that give the solver a fixed
+ * device-memory budget under their own allocator or must not call cudaMalloc/cudaFree (which synchronize
+ * the device). Its scratch is a fixed array inside the library, held by every GPU that loads it (192 KiB);
+ * ncells is limited to 8,388,608 (CSU_ERR_INPUT beyond). The first call on a device looks the scratch
+ * address up (cudaGetSymbolAddress) and should come before any stream capture on that device. Calls
+ * whose kernels overlap on one GPU share the scratch and race. */
+int csu_residual_norms_noalloc(const double* R, int nvar, int ncells, double* res, void* stream);
+
 /* Counters of the engine: kernels launched since creation, device bytes held. */
 int csu_stats(csu_ctx* ctx, long long* kernel_launches, long long* device_bytes);
 
