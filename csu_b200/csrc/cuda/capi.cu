@@ -159,6 +159,7 @@ static void plan(csu_ctx* x, Arena& a)
     s.GTx = carve<double>(a, visc ? nc : 0);
     s.GTy = carve<double>(a, visc ? nc : 0);
     s.FV = carve<double4>(a, visc ? (size_t)nf + nb : 0);
+    s.MIT = carve<double>(a, (x->cfg.sa || x->cfg.sst) ? nf : 0);
     s.Gxx = carve<double>(a, (size_t)nx * nc);
     s.Gxy = carve<double>(a, (size_t)nx * nc);
     s.PHx = carve<double>(a, (size_t)nx * nc);
@@ -310,6 +311,7 @@ static void fill_params(csu_ctx* x)
     const char* fast = getenv("CSU_LSQ_FAST");
     p.lsq_exact = (fast && fast[0] == '1') ? 0 : 1;
     p.visc = (c.laminar || c.sa || c.sst) ? 1 : 0;
+    p.visc_blazek = c.visc_blazek;
     p.conv_tol = 0;
 }
 
@@ -344,8 +346,13 @@ extern "C" int csu_create(const csu_mesh_desc* md, const csu_config* cfg, csu_ct
         csu_set_error("csu_create: nvar %d does not match the turbulence model", cfg->nvar);
         return CSU_ERR_INPUT;
     }
-    if (model != 0) {
-        csu_set_error("csu_create: turbulence models are not available in this engine build");
+    if (model == 2) {
+        csu_set_error("csu_create: the SST model is not available in this engine build");
+        return CSU_ERR_UNSUPPORTED;
+    }
+    if (model == 1 && (cfg->flux == CSU_FLUX_ROE || cfg->sa_cc)) {
+        csu_set_error("csu_create: SA with %s is not available (the reference has no Roe branch for SA)",
+                      cfg->sa_cc ? "saCC" : "Roe");
         return CSU_ERR_UNSUPPORTED;
     }
     if (cfg->time_scheme == CSU_TS_LUSGS) {

@@ -5,6 +5,7 @@
 #include "physics.cuh"
 #include "ext80.cuh"
 #include "viscous.cuh"
+#include "sa.cuh"
 
 namespace csu {
 
@@ -25,6 +26,7 @@ struct Prm {
     int order, scheme, laminar, sa, sst, axi, turb1order, limiter_type, stages, dt_local_n, tube, n_linear;
     int lsq_exact;      // gradients with the reference's x87 rounding (1) or precomputed FP64 weights (0)
     int visc;           // laminar, SA or SST: temperature gradient and viscous fluxes
+    int visc_blazek;    // SA face gradients with the directional correction (saInterFaceB)
     double lim_k, vol_max, e_fix, r_lim, p_out, t_wall, pr, pr_t, w_imp, cfl, sigma, mach_inf, sref;
     double pin[7];
     double pref20[6];   // limiterUpdate type 0 reference squares (limiter.c:49-59)
@@ -98,7 +100,8 @@ struct State {
     double4* W4;  double* WT;  double* Wx;    // primitives of the cells
     double4* G4x; double4* G4y; double4* PH4; // gradients and limiter (r u v p)
     double* GTx;  double* GTy;                // temperature gradient (solverGrad_T, viscous models)
-    double4* FV;                              // viscous face fluxes (x, y momentum, energy)
+    double4* FV;                              // viscous face fluxes (x, y momentum, energy, nt)
+    double* MIT;                              // face eddy viscosity of interior faces (SA, SST)
     double* Gxx;  double* Gxy;  double* PHx;  // same for the scalars, [k][cell]
     double4* F4;  double* Fx;                 // face fluxes * |dS|: nf interior then nb boundary
     double4* R4;  double* Rx;                 // residual

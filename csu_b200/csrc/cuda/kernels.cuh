@@ -259,7 +259,17 @@ __global__ void __launch_bounds__(BLOCK) k_flux(const __grid_constant__ Prm p, c
                 PR[kk] = B[slot2p(kk)];
             }
         }
-        if (p.laminar == 1) {
+        if constexpr (MODEL == 1) {
+            double4 a = s.G4x[e.x], b = s.G4y[e.x], cc = s.G4x[e.y], d = s.G4y[e.y];
+            double g0x[4] = {a.y, a.z, s.GTx[e.x], s.Gxx[e.x]}, g0y[4] = {b.y, b.z, s.GTy[e.x], s.Gxy[e.x]};
+            double g1x[4] = {cc.y, cc.z, s.GTx[e.y], s.Gxx[e.y]}, g1y[4] = {d.y, d.z, s.GTy[e.y], s.Gxy[e.y]};
+            double2 dd = m.fd[f];
+            double fv[4], mit;
+            sa_face_flux(p.gas, p.pr, p.pr_t, p.visc_blazek, g0x, g0y, g1x, g1y, A, B, dd.x, dd.y, m.fL[f], dSx,
+                         dSy, fv, &mit);
+            s.FV[f] = make_double4(fv[0], fv[1], fv[2], fv[3]);
+            s.MIT[f] = mit;
+        } else if (p.laminar == 1) {
             double4 a = s.G4x[e.x], b = s.G4y[e.x], cc = s.G4x[e.y], d = s.G4y[e.y];
             double g0x[3] = {a.y, a.z, s.GTx[e.x]}, g0y[3] = {b.y, b.z, s.GTy[e.x]};
             double g1x[3] = {cc.y, cc.z, s.GTx[e.y]}, g1y[3] = {d.y, d.z, s.GTy[e.y]};
@@ -293,17 +303,25 @@ __global__ void __launch_bounds__(BLOCK) k_flux(const __grid_constant__ Prm p, c
                           : make_double4(0.0, 0.0, 0.0, 0.0);
 #pragma unroll
         for (int kk = 4; kk < NV; kk++) s.Fx[(size_t)(kk - 4) * (m.nf + m.nb) + fi] = dS > 0 ? fl[kk] * sc : 0.0;
-        double gvx[3], gvy[3];
+        double gvx[4], gvy[4];
         double2 bdv = make_double2(0.0, 0.0);
         double bLv = 0.0;
         if (p.visc) {
             double4 a = s.G4x[c], bb = s.G4y[c];
             gvx[0] = a.y; gvx[1] = a.z; gvx[2] = s.GTx[c];
             gvy[0] = bb.y; gvy[1] = bb.z; gvy[2] = s.GTy[c];
+            gvx[3] = MODEL >= 1 ? s.Gxx[c] : 0.0;
+            gvy[3] = MODEL >= 1 ? s.Gxy[c] : 0.0;
             bdv = m.bd[b];
             bLv = m.bL[b];
         }
-        if (p.laminar == 1) {
+        if constexpr (MODEL == 1) {
+            double2 un = m.bun[b];
+            double fv[4];
+            sa_boundary_flux(p.gas, p.pr, p.pr_t, p.t_wall, p.pin, flag, gvx, gvy, E0, dSx, dSy, bdv.x, bdv.y, bLv,
+                             un.x, un.y, m.bds2[b], fv);
+            s.FV[fi] = make_double4(fv[0], fv[1], fv[2], fv[3]);
+        } else if (p.laminar == 1) {
             double2 un = m.bun[b];
             double fv[3];
             laminar_boundary(p.gas, p.pr, p.t_wall, p.pin, flag, gvx, gvy, E0, dSx, dSy, bdv.x, bdv.y, bLv, un.x,
@@ -360,24 +378,48 @@ __device__ __forceinline__ void gather_residual(const Prm& p, const Mesh& m, con
         R[2] -= P[3] * dS;
         if constexpr (MODEL == 2) R[2] -= (2. / 3.) * P[0] * P[5] * dS;
     }
-    if (p.laminar == 1) {
-        // laminarInter gather then laminarBoundary (laminar.c:77-125)
+    if (p.laminar == 1 || MODEL == 1) {
+        // laminarInter / saInter face gather (laminar.c:77-98, sa.c:197-220), the SA source (sa.c:224-256),
+        // then laminarBoundary / saBoundary (laminar.c:101-125, sa.c:351-368, 695-701)
         const int ni = m.nint[c];
 #pragma unroll
         for (int j = 0; j < 4; j++) {
-            if (j < ns) {
+            if (j < ni) {
                 int sf = m.fslot[(size_t)j * nc + c];
                 int fi = sf > 0 ? sf - 1 : -sf - 1;
                 double4 V = s.FV[fi];
-                if (j >= ni || sf > 0) {
+                if (sf > 0) {
                     R[1] -= V.x;
                     R[2] -= V.y;
                     R[3] -= V.z;
+                    if constexpr (MODEL == 1) R[4] -= V.w;
                 } else {
                     R[1] += V.x;
                     R[2] += V.y;
                     R[3] += V.z;
+                    if constexpr (MODEL == 1) R[4] += V.w;
                 }
+            }
+        }
+        if constexpr (MODEL == 1) {
+            double4 gx = s.G4x[c], gy = s.G4y[c];
+            double rho = P[0], T = P[4], n = P[5];
+            double d = m.wall_d[c];
+            double mi_L = sutherland(T);
+            double n_L = mi_L / rho;
+            double S = fabs(gy.y - gx.z);
+            double Qt = sa_source(n, n_L, S, d, rho, gx.x, gy.x, s.Gxx[c], s.Gxy[c]);
+            R[4] -= Qt * m.omega[c];
+        }
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+            if (j >= ni && j < ns) {
+                int fi = m.fslot[(size_t)j * nc + c] - 1;
+                double4 V = s.FV[fi];
+                R[1] -= V.x;
+                R[2] -= V.y;
+                R[3] -= V.z;
+                if constexpr (MODEL == 1) R[4] -= V.w;
             }
         }
     }
@@ -516,7 +558,11 @@ __global__ void __launch_bounds__(BLOCK) k_impl(const __grid_constant__ Prm p, c
             double cc = T2c(p.gas, T);
             double nx = dSv.x / dS, ny = dSv.y / dS;
             Lc += (fabs(nx * u + ny * v) + cc) * dS;
-            if (p.laminar) {
+            if constexpr (MODEL >= 1) {
+                double r = (w0.x + w1.x) * 0.5;
+                double mi = sutherland(T);
+                Lv += fmax(4 / (3 * r), T2gamma(p.gas, T) / r) * (mi / p.pr + s.MIT[f] / p.pr_t) * dS * dS;
+            } else if (p.laminar) {
                 double r = (w0.x + w1.x) * 0.5;
                 Lv += visc_radius(p.gas, p.pr, r, T) * dS * dS;
             }
@@ -588,7 +634,13 @@ __global__ void __launch_bounds__(BLOCK) k_impl(const __grid_constant__ Prm p, c
                 }
                 double cc = T2c(p.gas, Pn[4]);
                 double ra = p.w_imp * (fabs(nx * Pn[1] + ny * Pn[2]) + cc) * dS;
-                if (p.laminar) {
+                if constexpr (MODEL == 1) {
+                    // implicitUpdateA_sa (implicit.c:920-928): always viscous, with the face eddy viscosity
+                    double r = (P[0] + Pn[0]) * 0.5;
+                    double T = (P[4] + Pn[4]) * 0.5;
+                    double mi = sutherland(T);
+                    ra += fmax(4 / (3 * r), T2gamma(p.gas, T) / r) * (mi / p.pr + s.MIT[f] / p.pr_t) * dS / m.fL[f];
+                } else if (p.laminar) {
                     double r = (P[0] + Pn[0]) * 0.5;
                     double T = (P[4] + Pn[4]) * 0.5;
                     ra += visc_radius(p.gas, p.pr, r, T) * dS / m.fL[f];

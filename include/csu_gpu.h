@@ -128,6 +128,11 @@ int csu_case_get_double(const csu_case* c, const char* keyword, double* out);
 int csu_case_marker_name(const csu_case* c, int marker, char* out, int cap);
 void csu_case_free(csu_case* c);
 
+/* The whole program flow of the reference executable (main.c:18-45 with solverSolve, solver.c:1836-1943)
+ * on the engine: read <wd>, iterate Nmax times (or run the tube to tmax), and write convergence.csv,
+ * friction.csv, solution.csv, solution2.csv and restart.csv into <wd>. verbose prints like the reference. */
+int csu_run_case(const char* wd, int verbose);
+
 /* ------------------------------------------------------------------------------------------------
  * Device engine.
  * ---------------------------------------------------------------------------------------------- */
