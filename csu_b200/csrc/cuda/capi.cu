@@ -160,6 +160,7 @@ static void plan(csu_ctx* x, Arena& a)
     s.GTy = carve<double>(a, visc ? nc : 0);
     s.FV = carve<double4>(a, visc ? (size_t)nf + nb : 0);
     s.MIT = carve<double>(a, (x->cfg.sa || x->cfg.sst) ? nf : 0);
+    s.FV5 = carve<double>(a, x->cfg.sst ? (size_t)nf + nb : 0);
     s.Gxx = carve<double>(a, (size_t)nx * nc);
     s.Gxy = carve<double>(a, (size_t)nx * nc);
     s.PHx = carve<double>(a, (size_t)nx * nc);
@@ -305,6 +306,15 @@ static void fill_params(csu_ctx* x)
     p.p_inf = c.pin[3];
     p.q_inf = 0.5 * c.pin[0] * (c.pin[1] * c.pin[1] + c.pin[2] * c.pin[2]);
     p.sst_b1 = 0.075;
+    {
+        // sstInit (sst.c:18-39)
+        SstK& k = p.sst_k;
+        k.sk1 = 0.85; k.so1 = 0.5; k.b1 = 0.075; k.sk2 = 1.0; k.so2 = 0.856; k.b2 = 0.0828; k.bs = 0.09; k.a1 = 0.31;
+        double kap = 0.41;
+        k.g1 = k.b1 / k.bs - k.so1 * kap * kap / sqrt(k.bs);
+        k.g2 = k.b2 / k.bs - k.so2 * kap * kap / sqrt(k.bs);
+        k.o_wall_factor = c.o_wall_factor;
+    }
     p.o_wall_factor = c.o_wall_factor;
     p.tmax = 0;
     // exact x87 gradients unless CSU_LSQ_FAST=1 (FP64 weights: faster, last-bit differences)
@@ -346,8 +356,9 @@ extern "C" int csu_create(const csu_mesh_desc* md, const csu_config* cfg, csu_ct
         csu_set_error("csu_create: nvar %d does not match the turbulence model", cfg->nvar);
         return CSU_ERR_INPUT;
     }
-    if (model == 2) {
-        csu_set_error("csu_create: the SST model is not available in this engine build");
+    if (model == 2 && (cfg->flux == CSU_FLUX_ROE || cfg->sst_trans || cfg->time_scheme != CSU_TS_RK)) {
+        csu_set_error("csu_create: SST supports RK time stepping with the AUSM family (the reference has no Roe "
+                      "branch for SST and calls 4x4 DPLUR blocks with 6 variables); sstTrans not yet available");
         return CSU_ERR_UNSUPPORTED;
     }
     if (model == 1 && (cfg->flux == CSU_FLUX_ROE || cfg->sa_cc)) {

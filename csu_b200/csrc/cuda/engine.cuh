@@ -6,6 +6,7 @@
 #include "ext80.cuh"
 #include "viscous.cuh"
 #include "sa.cuh"
+#include "sst.cuh"
 
 namespace csu {
 
@@ -32,6 +33,7 @@ struct Prm {
     double pref20[6];   // limiterUpdate type 0 reference squares (limiter.c:49-59)
     double q_inf, p_inf;// solverCalcCoeff3 dynamic pressure and pressure (solver.c:1348-1352)
     double sst_b1, o_wall_factor;
+    SstK sst_k;         // SST constants (sstInit)
     double tmax;        // tube end time
     double conv_tol;    // stop when res[0] <= conv_tol * res0[0] (0: never)
 };
@@ -102,6 +104,7 @@ struct State {
     double* GTx;  double* GTy;                // temperature gradient (solverGrad_T, viscous models)
     double4* FV;                              // viscous face fluxes (x, y momentum, energy, nt)
     double* MIT;                              // face eddy viscosity of interior faces (SA, SST)
+    double* FV5;                              // SST: 5th viscous component (omega)
     double* Gxx;  double* Gxy;  double* PHx;  // same for the scalars, [k][cell]
     double4* F4;  double* Fx;                 // face fluxes * |dS|: nf interior then nb boundary
     double4* R4;  double* Rx;                 // residual

@@ -259,7 +259,20 @@ __global__ void __launch_bounds__(BLOCK) k_flux(const __grid_constant__ Prm p, c
                 PR[kk] = B[slot2p(kk)];
             }
         }
-        if constexpr (MODEL == 1) {
+        if constexpr (MODEL == 2) {
+            double4 a = s.G4x[e.x], b = s.G4y[e.x], cc = s.G4x[e.y], d = s.G4y[e.y];
+            double g0x[5] = {a.y, a.z, s.GTx[e.x], s.Gxx[e.x], s.Gxx[(size_t)nc + e.x]};
+            double g0y[5] = {b.y, b.z, s.GTy[e.x], s.Gxy[e.x], s.Gxy[(size_t)nc + e.x]};
+            double g1x[5] = {cc.y, cc.z, s.GTx[e.y], s.Gxx[e.y], s.Gxx[(size_t)nc + e.y]};
+            double g1y[5] = {d.y, d.z, s.GTy[e.y], s.Gxy[e.y], s.Gxy[(size_t)nc + e.y]};
+            double2 dd = m.fd[f];
+            double fv[5], mit;
+            sst_face_flux(p.gas, p.sst_k, p.pr, p.pr_t, g0x, g0y, g1x, g1y, A, B, m.wall_d[e.x], m.wall_d[e.y], dd.x,
+                          dd.y, m.fL[f], dSx, dSy, fv, &mit);
+            s.FV[f] = make_double4(fv[0], fv[1], fv[2], fv[3]);
+            s.FV5[f] = fv[4];
+            s.MIT[f] = mit;
+        } else if constexpr (MODEL == 1) {
             double4 a = s.G4x[e.x], b = s.G4y[e.x], cc = s.G4x[e.y], d = s.G4y[e.y];
             double g0x[4] = {a.y, a.z, s.GTx[e.x], s.Gxx[e.x]}, g0y[4] = {b.y, b.z, s.GTy[e.x], s.Gxy[e.x]};
             double g1x[4] = {cc.y, cc.z, s.GTx[e.y], s.Gxx[e.y]}, g1y[4] = {d.y, d.z, s.GTy[e.y], s.Gxy[e.y]};
@@ -303,7 +316,7 @@ __global__ void __launch_bounds__(BLOCK) k_flux(const __grid_constant__ Prm p, c
                           : make_double4(0.0, 0.0, 0.0, 0.0);
 #pragma unroll
         for (int kk = 4; kk < NV; kk++) s.Fx[(size_t)(kk - 4) * (m.nf + m.nb) + fi] = dS > 0 ? fl[kk] * sc : 0.0;
-        double gvx[4], gvy[4];
+        double gvx[5], gvy[5];
         double2 bdv = make_double2(0.0, 0.0);
         double bLv = 0.0;
         if (p.visc) {
@@ -312,10 +325,19 @@ __global__ void __launch_bounds__(BLOCK) k_flux(const __grid_constant__ Prm p, c
             gvy[0] = bb.y; gvy[1] = bb.z; gvy[2] = s.GTy[c];
             gvx[3] = MODEL >= 1 ? s.Gxx[c] : 0.0;
             gvy[3] = MODEL >= 1 ? s.Gxy[c] : 0.0;
+            gvx[4] = MODEL == 2 ? s.Gxx[(size_t)nc + c] : 0.0;
+            gvy[4] = MODEL == 2 ? s.Gxy[(size_t)nc + c] : 0.0;
             bdv = m.bd[b];
             bLv = m.bL[b];
         }
-        if constexpr (MODEL == 1) {
+        if constexpr (MODEL == 2) {
+            double2 un = m.bun[b];
+            double fv[5];
+            sst_boundary_flux(p.gas, p.sst_k, p.pr, p.pr_t, p.t_wall, p.pin, flag, gvx, gvy, E0, m.wall_d[c], dSx,
+                              dSy, bdv.x, bdv.y, bLv, un.x, un.y, m.bds2[b], fv);
+            s.FV[fi] = make_double4(fv[0], fv[1], fv[2], fv[3]);
+            s.FV5[fi] = fv[4];
+        } else if constexpr (MODEL == 1) {
             double2 un = m.bun[b];
             double fv[4];
             sa_boundary_flux(p.gas, p.pr, p.pr_t, p.t_wall, p.pin, flag, gvx, gvy, E0, dSx, dSy, bdv.x, bdv.y, bLv,
@@ -378,7 +400,7 @@ __device__ __forceinline__ void gather_residual(const Prm& p, const Mesh& m, con
         R[2] -= P[3] * dS;
         if constexpr (MODEL == 2) R[2] -= (2. / 3.) * P[0] * P[5] * dS;
     }
-    if (p.laminar == 1 || MODEL == 1) {
+    if (p.laminar == 1 || MODEL >= 1) {
         // laminarInter / saInter face gather (laminar.c:77-98, sa.c:197-220), the SA source (sa.c:224-256),
         // then laminarBoundary / saBoundary (laminar.c:101-125, sa.c:351-368, 695-701)
         const int ni = m.nint[c];
@@ -392,12 +414,14 @@ __device__ __forceinline__ void gather_residual(const Prm& p, const Mesh& m, con
                     R[1] -= V.x;
                     R[2] -= V.y;
                     R[3] -= V.z;
-                    if constexpr (MODEL == 1) R[4] -= V.w;
+                    if constexpr (MODEL >= 1) R[4] -= V.w;
+                    if constexpr (MODEL == 2) R[5] -= s.FV5[fi];
                 } else {
                     R[1] += V.x;
                     R[2] += V.y;
                     R[3] += V.z;
-                    if constexpr (MODEL == 1) R[4] += V.w;
+                    if constexpr (MODEL >= 1) R[4] += V.w;
+                    if constexpr (MODEL == 2) R[5] += s.FV5[fi];
                 }
             }
         }
@@ -411,6 +435,17 @@ __device__ __forceinline__ void gather_residual(const Prm& p, const Mesh& m, con
             double Qt = sa_source(n, n_L, S, d, rho, gx.x, gy.x, s.Gxx[c], s.Gxy[c]);
             R[4] -= Qt * m.omega[c];
         }
+        if constexpr (MODEL == 2) {
+            double4 gx = s.G4x[c], gy = s.G4y[c];
+            double sgx[4] = {gx.y, gx.z, s.Gxx[c], s.Gxx[(size_t)nc + c]};
+            double sgy[4] = {gy.y, gy.z, s.Gxy[c], s.Gxy[(size_t)nc + c]};
+            double Qtk, Qto;
+            sst_cell_source(p.sst_k, sgx, sgy, P, m.wall_d[c], &Qtk, &Qto);
+            if (P[6] != 0.0) {
+                R[4] -= Qtk * m.omega[c];
+                R[5] -= Qto * m.omega[c];
+            }
+        }
 #pragma unroll
         for (int j = 0; j < 4; j++) {
             if (j >= ni && j < ns) {
@@ -419,7 +454,8 @@ __device__ __forceinline__ void gather_residual(const Prm& p, const Mesh& m, con
                 R[1] -= V.x;
                 R[2] -= V.y;
                 R[3] -= V.z;
-                if constexpr (MODEL == 1) R[4] -= V.w;
+                if constexpr (MODEL >= 1) R[4] -= V.w;
+                if constexpr (MODEL == 2) R[5] -= s.FV5[fi];
             }
         }
     }
