@@ -52,6 +52,7 @@ struct csu_ctx {
     const double* rk = nullptr;
     cudaGraphExec_t graph = nullptr;
     int graph_iters = 0;
+    long long graph_launches = 0;
     int have_debug = 0;
     cudaStream_t own_stream = nullptr;
     // kernel timing (csu_time_kernels): an event after every launch, tagged with the kernel kind
@@ -145,6 +146,8 @@ static void plan(csu_ctx* x, Arena& a)
     m.bL = carve<double>(a, nb);
     m.bun = carve<double2>(a, nb);
     m.bds2 = carve<double>(a, nb);
+    m.color = carve<int>(a, nc);
+    m.color_cells = carve<int>(a, nc);
     x->d_wall_rank = carve<int>(a, nb);
 
     s.U4 = carve<double4>(a, nc);
@@ -253,6 +256,8 @@ static int upload_mesh(csu_ctx* x)
     CK(up(m.bL, L.bL, sizeof(double) * nb));
     CK(up(m.bun, bun.data(), sizeof(double2) * nb));
     CK(up(m.bds2, L.bds2, sizeof(double) * nb));
+    CK(up(m.color, L.color, sizeof(int) * nc));
+    CK(up(m.color_cells, L.color_cells, sizeof(int) * nc));
     CK(up(x->d_wall_rank, rank.data(), sizeof(int) * nb));
     return CSU_OK;
 }
@@ -366,8 +371,8 @@ extern "C" int csu_create(const csu_mesh_desc* md, const csu_config* cfg, csu_ct
                       cfg->sa_cc ? "saCC" : "Roe");
         return CSU_ERR_UNSUPPORTED;
     }
-    if (cfg->time_scheme == CSU_TS_LUSGS) {
-        csu_set_error("csu_create: LU-SGS is not available in this engine build");
+    if (cfg->time_scheme == CSU_TS_LUSGS && model == 2) {
+        csu_set_error("csu_create: LU-SGS with SST is not available in this engine build");
         return CSU_ERR_UNSUPPORTED;
     }
     if (cfg->time_scheme == CSU_TS_RK && !(cfg->stages == 1 || cfg->stages == 3 || cfg->stages == 4 ||
@@ -564,6 +569,32 @@ static void launch_iteration(csu_ctx* x)
             tmark(x, KRK);
         }
         launch_finalize<MODEL>(x, 0);
+    } else if (c.time_scheme == CSU_TS_LUSGS) {
+        if (c.order == 2 || x->prm.visc) launch_grad<MODEL>(x, false);
+        launch_flux<MODEL>(x, 1);
+        k_impl<MODEL, false><<<x->gb_c, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st);
+        x->launches++;
+        tmark(x, KIMPL);
+        const int K = x->L.ncolors;
+        for (int pass = 0; pass < 2; pass++)
+            for (int q = 0; q < K; q++) {
+                int col = pass == 0 ? q : K - 1 - q;
+                int start = x->L.color_start[col], count = x->L.color_start[col + 1] - start;
+                if (count == 0) continue;
+                int g = (count + BLOCK - 1) / BLOCK;
+                if (pass == 0)
+                    k_lusgs<MODEL, true><<<g, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st, x->mesh.color,
+                                                                     x->mesh.color_cells, col, start, count);
+                else
+                    k_lusgs<MODEL, false><<<g, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st, x->mesh.color,
+                                                                      x->mesh.color_cells, col, start, count);
+                x->launches++;
+                tmark(x, KSWEEP);
+            }
+        k_update<MODEL><<<x->gb_c, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st);
+        x->launches++;
+        tmark(x, KPRIM);
+        launch_finalize<MODEL>(x, 1);
     } else {
         if (c.order == 2 || x->prm.visc) launch_grad<MODEL>(x, false);
         launch_flux<MODEL>(x, 1);
@@ -643,6 +674,7 @@ static int build_graph(csu_ctx* x, int iters)
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
     x->graph_iters = iters;
+    x->graph_launches = x->launches - l0;
     x->xcur = xcur0;
     x->launches = l0;
     return CSU_OK;
@@ -674,9 +706,7 @@ static int run_iterations(csu_ctx* x, int n, int it0, Scalars* out)
             if ((st = build_graph(x, G))) return st;
         while (n - done >= G) {
             CK(cudaGraphLaunch(x->graph, x->stream));
-            int per = x->cfg.time_scheme == CSU_TS_RK ? x->cfg.stages * (x->cfg.order == 2 ? 3 : 2) + 1
-                                                       : (x->cfg.order == 2 ? 3 : 2) + x->cfg.n_linear + 1;
-            x->launches += (long long)per * G;
+            x->launches += x->graph_launches;
             done += G;
         }
     }

@@ -95,6 +95,8 @@ struct Mesh {
     const double* bL;               // |bd|
     const double2* bun;             // unit normal of meshCalcDS2 (unscaled)
     const double* bds2;             // |dS| of meshCalcDS2 (axisymmetric: times the mean y)
+    const int* color;               // cell colour (LU-SGS)
+    const int* color_cells;         // cells grouped by colour
 };
 
 struct State {

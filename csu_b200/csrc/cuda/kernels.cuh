@@ -777,6 +777,160 @@ __global__ void __launch_bounds__(BLOCK) k_sweep(const __grid_constant__ Prm p, 
     }
 }
 
+// implicitCalcDeltaFlux (implicit.c:194-231) and implicitCalcDeltaFlux_sa (495-552): F(U + d) - F(U) on the
+// face normal, from the neighbour's primitives P and increment d.
+template <int MODEL>
+__device__ __forceinline__ void delta_flux(const Prm& p, const double* P, const double* d, double nx, double ny,
+                                           double* dF)
+{
+    constexpr int NV = Model<MODEL>::NV;
+    double rho = P[0], u = P[1], v = P[2], pr = P[3];
+    double U[NV], F0[NV], F1[NV];
+    double T = pr / (p.gas.R * rho);
+    double e0 = T2e(p.gas, T);
+    double E = e0 + (u * u + v * v) / 2;
+    U[0] = rho;
+    U[1] = rho * u;
+    U[2] = rho * v;
+    U[3] = rho * E;
+    if constexpr (MODEL == 1) U[4] = rho * P[5];
+    aux_flux<NV>(U, pr, nx, ny, F0);
+#pragma unroll
+    for (int k = 0; k < NV; k++) U[k] = U[k] + d[k];
+    if constexpr (MODEL == 0) {
+        rho = U[0];
+        u = U[1] / rho;
+        v = U[2] / rho;
+        E = U[3] / rho;
+        double e1 = E - 0.5 * (u * u + v * v);
+        T = e2Taprox(p.gas, e0, T, e1);
+        pr = p.gas.R * T * rho;
+    } else {
+        rho = U[0];
+        rho = fmax(rho, p.r_lim);
+        U[0] = rho;
+        u = U[1] / rho;
+        v = U[2] / rho;
+        E = U[3] / rho;
+        double e1 = E - (u * u + v * v) * 0.5;
+        e1 = fmax(e1, 7.176325e+02);
+        T = e2Taprox(p.gas, e0, T, e1);
+        if (T < 1) {
+            T = 1;
+            e1 = T2e(p.gas, T);
+            E = e1 + (u * u + v * v) * 0.5;
+            U[3] = rho * E;
+        }
+        pr = p.gas.R * T * rho;
+        double n = U[4] / rho;
+        n = fmax(n, 0);
+        U[4] = rho * n;
+    }
+    aux_flux<NV>(U, pr, nx, ny, F1);
+#pragma unroll
+    for (int k = 0; k < NV; k++) dF[k] = F1[k] - F0[k];
+}
+
+// ------------------------------------------------------------------------------------------------
+// k_lusgs: one colour of the LU-SGS sweeps (implicitLUSGS_L / _U, implicit.c:274-482) as a multicolour
+// Gauss-Seidel: the reference sweeps cells in index order using the already-updated lower (upper) index
+// neighbours; here the cells of one colour update together using the neighbours of lower (higher) colours.
+// Same operator, another ordering: the converged solution is the same, the path to it is not.
+//   FWD: x0_i = (-R_i - sum_{lower} 0.5 (dF(x0_j) dS - ra_j x0_j)) / D_i
+//   BWD: x1_i = (D_i x0_i - sum_{higher} 0.5 (dF(x1_j) dS - ra_j x1_j)) / D_i
+// ------------------------------------------------------------------------------------------------
+template <int MODEL, bool FWD>
+__global__ void __launch_bounds__(BLOCK) k_lusgs(const __grid_constant__ Prm p, const __grid_constant__ Mesh m,
+                                                 const __grid_constant__ State s, const int* color,
+                                                 const int* cells, int mycolor, int start, int count)
+{
+    constexpr int NV = Model<MODEL>::NV, NP = Model<MODEL>::NP;
+    if (halted(s)) return;
+    int t = blockIdx.x * BLOCK + threadIdx.x;
+    if (t >= count) return;
+    const int nc = m.nc;
+    int c = cells[start + t];
+    const double4* src4 = FWD ? s.X4[0] : s.X4[1];
+    const double* srcx = FWD ? s.Xx[0] : s.Xx[1];
+    double dt = bitsd(s.sc->dtmin_bits) * p.cfl;
+    double D = s.dpart[c] + m.omega[c] / dt;
+    double x[NV];
+    if (FWD) {
+        double4 t4 = s.R4[c];
+        x[0] = -t4.x; x[1] = -t4.y; x[2] = -t4.z; x[3] = -t4.w;
+#pragma unroll
+        for (int k = 4; k < NV; k++) x[k] = -s.Rx[(size_t)(k - 4) * nc + c];
+    } else {
+        double4 t4 = s.X4[0][c];
+        x[0] = D * t4.x; x[1] = D * t4.y; x[2] = D * t4.z; x[3] = D * t4.w;
+#pragma unroll
+        for (int k = 4; k < NV; k++) x[k] = D * s.Xx[0][(size_t)(k - 4) * nc + c];
+    }
+    double P0[NP];
+    loadP<MODEL>(s, nc, c, P0);
+    const int ni = m.nint[c];
+    for (int j = 0; j < ni; j++) {
+        int sf = m.fslot[(size_t)j * nc + c];
+        int f = sf > 0 ? sf - 1 : -sf - 1;
+        int2 e = m.fe[f];
+        int nb = sf > 0 ? e.y : e.x;
+        int cn = color[nb];
+        if (FWD ? (cn >= mycolor) : (cn <= mycolor)) continue;
+        double2 dSv = m.fn[f];
+        double dSx = sf > 0 ? dSv.x : -dSv.x, dSy = sf > 0 ? dSv.y : -dSv.y;
+        double dS = m.fds[f];
+        double nx = dSx / dS, ny = dSy / dS;
+        double Pn[NP], dn[NV], dF[NV];
+        loadP<MODEL>(s, nc, nb, Pn);
+        {
+            double4 t4 = src4[nb];
+            dn[0] = t4.x; dn[1] = t4.y; dn[2] = t4.z; dn[3] = t4.w;
+#pragma unroll
+            for (int k = 4; k < NV; k++) dn[k] = srcx[(size_t)(k - 4) * nc + nb];
+        }
+        delta_flux<MODEL>(p, Pn, dn, nx, ny, dF);
+        double cc = T2c(p.gas, Pn[4]);
+        double ra = p.w_imp * (fabs(nx * Pn[1] + ny * Pn[2]) + cc) * dS;
+        if constexpr (MODEL == 1) {
+            double r = Pn[0], T = Pn[4];
+            double mi = sutherland(T);
+            ra += fmax(4 / (3 * r), T2gamma(p.gas, T) / r) * (mi / p.pr + s.MIT[f] / p.pr_t) * dS / m.fL[f];
+        } else if (p.laminar) {
+            ra += visc_radius(p.gas, p.pr, Pn[0], Pn[4]) * dS / m.fL[f];
+        }
+#pragma unroll
+        for (int k = 0; k < NV; k++) x[k] -= 0.5 * (dF[k] * dS - ra * dn[k]);
+    }
+#pragma unroll
+    for (int k = 0; k < NV; k++) x[k] /= D;
+    double4* dst4 = FWD ? s.X4[0] : s.X4[1];
+    double* dstx = FWD ? s.Xx[0] : s.Xx[1];
+    dst4[c] = make_double4(x[0], x[1], x[2], x[3]);
+#pragma unroll
+    for (int k = 4; k < NV; k++) dstx[(size_t)(k - 4) * nc + c] = x[k];
+}
+
+// U += dW1 (solverUpdateUImplicit), then the next iteration's primitives and clamps
+template <int MODEL>
+__global__ void __launch_bounds__(BLOCK) k_update(const __grid_constant__ Prm p, const __grid_constant__ Mesh m,
+                                                  const __grid_constant__ State s)
+{
+    constexpr int NV = Model<MODEL>::NV, NP = Model<MODEL>::NP;
+    if (halted(s)) return;
+    int c = blockIdx.x * BLOCK + threadIdx.x;
+    if (c >= m.nc) return;
+    const int nc = m.nc;
+    double U[NV], P[NP];
+    loadU<MODEL>(s, nc, c, U);
+    double4 t4 = s.X4[1][c];
+    U[0] += t4.x; U[1] += t4.y; U[2] += t4.z; U[3] += t4.w;
+#pragma unroll
+    for (int k = 4; k < NV; k++) U[k] += s.Xx[1][(size_t)(k - 4) * nc + c];
+    clamp_prim<MODEL>(p, U, P);
+    storeU<MODEL>(s, nc, c, U);
+    storeP<MODEL>(s, nc, c, P);
+}
+
 // ------------------------------------------------------------------------------------------------
 // k_finalize: one block closing an iteration (solverCalcRes, solverCalcCoeff3, history row, flags) and
 // preparing the next step size. mode: 0 RK iteration, 1 implicit iteration, 2 prologue (step size only),

@@ -115,7 +115,8 @@ void csu_layout_free(csu_layout* L)
                     L->fslot, L->omega, L->sxh, L->syh, L->xc, L->yc, L->wall_d, L->dslat, L->fe0, L->fe1,
                     L->fdsx, L->fdsy, L->fds, L->r0x, L->r0y, L->r1x, L->r1y, L->fdist, L->bown, L->bflag,
                     L->bold, L->bdsx, L->bdsy, L->bds, L->bmx, L->bmy, L->ldx, L->ldy, L->lm, L->les, L->lrv,
-                    L->fdx, L->fdy, L->bdx, L->bdy, L->bL, L->bunx, L->buny, L->bds2};
+                    L->fdx, L->fdy, L->bdx, L->bdy, L->bL, L->bunx, L->buny, L->bds2, L->color,
+                    L->color_start, L->color_cells};
     for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); i++) free(ptrs[i]);
     memset(L, 0, sizeof(*L));
 }
@@ -356,6 +357,32 @@ int csu_layout_build(const csu_mesh_desc* m, int axi, csu_layout* L)
         }
         L->fslot[(size_t)ns * nc + c] = nf + bn + 1;
         L->nslot[c] = ns + 1;
+    }
+    /* greedy colouring in the renumbered (Hilbert) order: the multicolour Gauss-Seidel of LU-SGS */
+    L->color = malloc(sizeof(int) * (nc > 0 ? nc : 1));
+    L->ncolors = 0;
+    for (int c = 0; c < nc; c++) {
+        unsigned used = 0;
+        for (int j = 0; j < L->nint[c]; j++) {
+            int sf = L->fslot[(size_t)j * nc + c];
+            int f = sf > 0 ? sf - 1 : -sf - 1;
+            int nb = sf > 0 ? L->fe1[f] : L->fe0[f];
+            if (nb < c) used |= 1u << L->color[nb];
+        }
+        int k = 0;
+        while (used & (1u << k)) k++;
+        L->color[c] = k;
+        if (k + 1 > L->ncolors) L->ncolors = k + 1;
+    }
+    L->color_start = calloc(L->ncolors + 1, sizeof(int));
+    L->color_cells = malloc(sizeof(int) * (nc > 0 ? nc : 1));
+    for (int c = 0; c < nc; c++) L->color_start[L->color[c] + 1]++;
+    for (int k = 0; k < L->ncolors; k++) L->color_start[k + 1] += L->color_start[k];
+    {
+        int* fill = malloc(sizeof(int) * (L->ncolors + 1));
+        memcpy(fill, L->color_start, sizeof(int) * (L->ncolors + 1));
+        for (int c = 0; c < nc; c++) L->color_cells[fill[L->color[c]]++] = c;
+        free(fill);
     }
     free(cx);
     free(cy);

@@ -76,6 +76,11 @@ typedef struct csu_layout {
     double* buny;
     double* bds2;
 
+    int* color;    /* greedy colouring of the cell graph (no two face neighbours share a colour)         */
+    int ncolors;
+    int* color_start;/* [ncolors + 1] ranges into color_cells                                         */
+    int* color_cells;/* cells grouped by colour, ascending within a colour                            */
+
     double vol_max;/* max omega (limiterUpdate type 0, limiter.c:44-48)                               */
     int max_npts;
 } csu_layout;
