@@ -46,7 +46,8 @@ class Config(C.Structure):
                                   "e_fix", "pr", "pr_t", "gamma", "gas_r")] + [
         ("pin", C.c_double * 7), ("uin", C.c_double * 6), ("mach_inf", C.c_double), ("inlet_p", C.c_double),
         ("inlet_t", C.c_double), ("sst_l", C.c_double), ("k_factor", C.c_double), ("o_factor", C.c_double),
-        ("o_wall_factor", C.c_double)]
+        ("o_wall_factor", C.c_double), ("implicit_fp32", C.c_int), ("implicit_local_dt", C.c_int),
+        ("cfl_ramp_iters", C.c_int), ("cfl_max", C.c_double), ("conv_drop", C.c_double)]
 
 
 class MeshDesc(C.Structure):
@@ -87,6 +88,7 @@ def lib():
         L.csu_get_state.argtypes = [vp, vp]
         L.csu_residual.argtypes = [vp, vp]
         L.csu_iterate.argtypes = [vp, C.c_int, C.c_int, vp]
+        L.csu_iterate_ex.argtypes = [vp, C.c_int, C.c_int, vp, ip]
         L.csu_tube_run.argtypes = [vp, C.c_double, ip, dp]
         L.csu_dump.argtypes = [vp, C.c_int, vp]
         L.csu_stats.argtypes = [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
@@ -210,6 +212,13 @@ class Engine:
         hist = np.zeros((max(n, 1), self.nvar + 4))
         _check(lib().csu_iterate(self._h, n, it0, _ptr(hist)))
         return hist[:n]
+
+    def iterate_until(self, n, it0=0):
+        """Up to n iterations, stopping at the convergence criterion; returns the history rows run."""
+        hist = np.zeros((max(n, 1), self.nvar + 4))
+        done = C.c_int()
+        _check(lib().csu_iterate_ex(self._h, n, it0, _ptr(hist), C.byref(done)))
+        return hist[:done.value]
 
     def tube_run(self, tmax):
         steps, t = C.c_int(), C.c_double()

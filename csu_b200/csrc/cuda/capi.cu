@@ -178,7 +178,9 @@ static void plan(csu_ctx* x, Arena& a)
         s.X4[k] = implicit ? carve<double4>(a, nc) : nullptr;
         s.Xx[k] = implicit ? carve<double>(a, (size_t)nx * nc) : nullptr;
     }
-    s.blocks = x->cfg.time_scheme == CSU_TS_DPLUR ? carve<double>(a, c4 * nv * nv) : nullptr;
+    bool dplur = x->cfg.time_scheme == CSU_TS_DPLUR;
+    s.blocks = dplur && !x->cfg.implicit_fp32 ? carve<double>(a, c4 * nv * nv) : nullptr;
+    s.blocks32 = dplur && x->cfg.implicit_fp32 ? carve<float>(a, c4 * nv * nv) : nullptr;
     s.part = carve<double>(a, (size_t)((nc + BLOCK - 1) / BLOCK) * nv);
     s.bcoef = carve<double>(a, (size_t)4 * (nb > 0 ? nb : 1));
     s.sc = carve<Scalars>(a, 1);
@@ -327,7 +329,11 @@ static void fill_params(csu_ctx* x)
     p.lsq_exact = (fast && fast[0] == '1') ? 0 : 1;
     p.visc = (c.laminar || c.sa || c.sst) ? 1 : 0;
     p.visc_blazek = c.visc_blazek;
-    p.conv_tol = 0;
+    p.conv_tol = c.conv_drop;
+    p.blk32 = c.implicit_fp32;
+    p.implicit_local_dt = c.implicit_local_dt;
+    p.cfl_ramp_iters = c.cfl_ramp_iters;
+    p.cfl_max = c.cfl_ramp_iters > 0 ? c.cfl_max : c.cfl;
 }
 
 static int reset_scalars(csu_ctx* x, int it0)
@@ -716,12 +722,14 @@ static int run_iterations(csu_ctx* x, int n, int it0, Scalars* out)
     return CSU_OK;
 }
 
-extern "C" int csu_iterate(csu_ctx* x, int n, int it0, double* hist)
+extern "C" int csu_iterate_ex(csu_ctx* x, int n, int it0, double* hist, int* n_done)
 {
     if (!x || n < 0) return CSU_ERR_INPUT;
+    if (n_done) *n_done = 0;
     if (n == 0) return CSU_OK;
     Scalars h;
     int st = run_iterations(x, n, it0, &h);
+    if (!st && n_done) *n_done = h.steps;
     if (st) return st;
     if (hist) {
         int rows = h.hist_row < n ? h.hist_row : n;
@@ -732,6 +740,11 @@ extern "C" int csu_iterate(csu_ctx* x, int n, int it0, double* hist)
         return h.status;
     }
     return CSU_OK;
+}
+
+extern "C" int csu_iterate(csu_ctx* x, int n, int it0, double* hist)
+{
+    return csu_iterate_ex(x, n, it0, hist, nullptr);
 }
 
 extern "C" int csu_tube_run(csu_ctx* x, double tmax, int* steps, double* t_final)
@@ -882,12 +895,18 @@ extern "C" int csu_dump(csu_ctx* x, int what, double* out)
         return CSU_OK;
     }
     case CSU_DUMP_BLOCKS: {
-        if (!x->st.blocks) {
+        if (!x->st.blocks && !x->st.blocks32) {
             csu_set_error("csu_dump: no DPLUR blocks in this context");
             return CSU_ERR_STATE;
         }
         size_t per = (size_t)nv * nv;
-        CK(d2h(a, x->st.blocks, (size_t)4 * per * nc));
+        if (x->st.blocks) {
+            CK(d2h(a, x->st.blocks, (size_t)4 * per * nc));
+        } else {
+            std::vector<float> f((size_t)4 * per * nc);
+            CK(cudaMemcpy(f.data(), x->st.blocks32, sizeof(float) * f.size(), cudaMemcpyDeviceToHost));
+            a.assign(f.begin(), f.end());
+        }
         for (int c = 0; c < nc; c++) {
             double* o = out + (size_t)n2o[c] * 4 * per;
             for (int j = 0; j < 4; j++)

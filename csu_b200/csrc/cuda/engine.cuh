@@ -36,6 +36,10 @@ struct Prm {
     SstK sst_k;         // SST constants (sstInit)
     double tmax;        // tube end time
     double conv_tol;    // stop when res[0] <= conv_tol * res0[0] (0: never)
+    int blk32;          // DPLUR blocks in FP32
+    int implicit_local_dt;
+    int cfl_ramp_iters; // CFL ramp (0: constant CFL)
+    double cfl_max;
 };
 
 // Device scalars updated by the kernels themselves (one per solve).
@@ -114,6 +118,7 @@ struct State {
     double* dpart;                            // implicit diagonal before Omega/dt
     double4* X4[2]; double* Xx[2];            // DPLUR increments (ping-pong)
     double* blocks;                           // DPLUR blocks [(slot*NV + row)*NV + col][cell]
+    float* blocks32;                          // the same in FP32 (mixed-precision DPLUR)
     double* part;                             // per-block partial sums of R^2 [block][NV]
     double* bcoef;                            // per reference boundary face: cp dSx, cp dSy, fx/q, fy/q
     double* hist;                             // history rows
@@ -180,6 +185,14 @@ __device__ __forceinline__ void storeP(const State& s, int nc, int i, const doub
     s.WT[i] = P[4];
 #pragma unroll
     for (int k = 5; k < Model<MODEL>::NP; k++) s.Wx[(size_t)(k - 5) * nc + i] = P[k];
+}
+
+// CFL of iteration `it`: the reference's constant CFL, or the geometric ramp extension
+__device__ __forceinline__ double cfl_at(const Prm& p, int it)
+{
+    if (p.cfl_ramp_iters <= 0) return p.cfl;
+    double f = it >= p.cfl_ramp_iters ? 1.0 : (double)it / p.cfl_ramp_iters;
+    return p.cfl * pow(p.cfl_max / p.cfl, f);
 }
 
 // primitive index of gradient/limiter slot kk (solver.c:461-468, 515-522)

@@ -40,7 +40,7 @@ __global__ void __launch_bounds__(BLOCK) k_prim(const __grid_constant__ Prm p, c
         loadU<MODEL>(s, m.nc, c, U);
         if (with_dt) {
             double l = local_step<MODEL>(p, U, m.sxh[c], m.syh[c], m.omega[c]);
-            s.dtl[c] = p.cfl * l;
+            s.dtl[c] = cfl_at(p, s.sc->iter) * l;
             lmin = l;
         }
         clamp_prim<MODEL>(p, U, P);
@@ -528,7 +528,7 @@ __global__ void __launch_bounds__(BLOCK) k_rk(const __grid_constant__ Prm p, con
         for (int k = 0; k < NV; k++) U[k] = U[k] - dt * p.sigma * a * R[k] / om;
         if (LAST) {
             double l = local_step<MODEL>(p, U, m.sxh[c], m.syh[c], om);
-            s.dtl[c] = p.cfl * l;
+            s.dtl[c] = cfl_at(p, s.sc->iter + 1) * l;
             lmin = l;
             clamp_prim<MODEL>(p, U, P);
             storeU<MODEL>(s, m.nc, c, U);
@@ -652,7 +652,7 @@ __global__ void __launch_bounds__(BLOCK) k_impl(const __grid_constant__ Prm p, c
                 double E = Un[3] / rho;
                 aux_flux<NV>(Un, Pn[3], nx, ny, F0);
                 double ee0 = E - 0.5 * (uu * uu + vv * vv);
-                double* A = s.blocks + (size_t)j * NV * NV * nc + c;
+                double A[NV * NV];
 #pragma unroll
                 for (int mm = 0; mm < NV; mm++) {
 #pragma unroll
@@ -666,7 +666,7 @@ __global__ void __launch_bounds__(BLOCK) k_impl(const __grid_constant__ Prm p, c
                     double pr = p.gas.R * r2 * T;
                     aux_flux<NV>(Uq, pr, nx, ny, F);
 #pragma unroll
-                    for (int nn = 0; nn < NV; nn++) A[(size_t)(nn * NV + mm) * nc] = 0.5 * (F[nn] - F0[nn]) * dS / h;
+                    for (int nn = 0; nn < NV; nn++) A[nn * NV + mm] = 0.5 * (F[nn] - F0[nn]) * dS / h;
                 }
                 double cc = T2c(p.gas, Pn[4]);
                 double ra = p.w_imp * (fabs(nx * Pn[1] + ny * Pn[2]) + cc) * dS;
@@ -682,7 +682,15 @@ __global__ void __launch_bounds__(BLOCK) k_impl(const __grid_constant__ Prm p, c
                     ra += visc_radius(p.gas, p.pr, r, T) * dS / m.fL[f];
                 }
 #pragma unroll
-                for (int nn = 0; nn < NV; nn++) A[(size_t)(nn * NV + nn) * nc] -= 0.5 * ra;
+                for (int nn = 0; nn < NV; nn++) A[nn * NV + nn] -= 0.5 * ra;
+                const size_t base = (size_t)j * NV * NV * nc + c;
+                if (p.blk32) {
+#pragma unroll
+                    for (int q = 0; q < NV * NV; q++) s.blocks32[base + (size_t)q * nc] = (float)A[q];
+                } else {
+#pragma unroll
+                    for (int q = 0; q < NV * NV; q++) s.blocks[base + (size_t)q * nc] = A[q];
+                }
             }
         }
     }
@@ -724,7 +732,8 @@ __global__ void __launch_bounds__(BLOCK) k_sweep(const __grid_constant__ Prm p, 
 #pragma unroll
             for (int k = 0; k < NV; k++) xn[k] = xo[k];
         } else {
-            double dt = bitsd(s.sc->dtmin_bits) * p.cfl;
+            double cfl = cfl_at(p, s.sc->iter);
+            double dt = p.implicit_local_dt ? s.dtl[c] * cfl : bitsd(s.sc->dtmin_bits) * cfl;
             double D = s.dpart[c] + m.omega[c] / dt;
             double y[NV];
 #pragma unroll
@@ -740,11 +749,20 @@ __global__ void __launch_bounds__(BLOCK) k_sweep(const __grid_constant__ Prm p, 
                 xb[0] = t.x; xb[1] = t.y; xb[2] = t.z; xb[3] = t.w;
 #pragma unroll
                 for (int k = 4; k < NV; k++) xb[k] = xox[(size_t)(k - 4) * nc + nb];
-                const double* A = s.blocks + (size_t)j * NV * NV * nc + c;
+                const size_t base = (size_t)j * NV * NV * nc + c;
+                if (p.blk32) {
+                    const float* A = s.blocks32 + base;
 #pragma unroll
-                for (int kk = 0; kk < NV; kk++)
+                    for (int kk = 0; kk < NV; kk++)
 #pragma unroll
-                    for (int nn = 0; nn < NV; nn++) y[kk] += A[(size_t)(kk * NV + nn) * nc] * xb[nn];
+                        for (int nn = 0; nn < NV; nn++) y[kk] += (double)A[(size_t)(kk * NV + nn) * nc] * xb[nn];
+                } else {
+                    const double* A = s.blocks + base;
+#pragma unroll
+                    for (int kk = 0; kk < NV; kk++)
+#pragma unroll
+                        for (int nn = 0; nn < NV; nn++) y[kk] += A[(size_t)(kk * NV + nn) * nc] * xb[nn];
+                }
             }
             double R[NV];
             {
@@ -852,7 +870,8 @@ __global__ void __launch_bounds__(BLOCK) k_lusgs(const __grid_constant__ Prm p, 
     int c = cells[start + t];
     const double4* src4 = FWD ? s.X4[0] : s.X4[1];
     const double* srcx = FWD ? s.Xx[0] : s.Xx[1];
-    double dt = bitsd(s.sc->dtmin_bits) * p.cfl;
+    double cfl = cfl_at(p, s.sc->iter);
+    double dt = p.implicit_local_dt ? s.dtl[c] * cfl : bitsd(s.sc->dtmin_bits) * cfl;
     double D = s.dpart[c] + m.omega[c] / dt;
     double x[NV];
     if (FWD) {
@@ -1000,7 +1019,7 @@ __global__ void __launch_bounds__(BLOCK) k_finalize(const __grid_constant__ Prm 
     if (mode == 0 || mode == 2) {
         // solverCalcDt (solver.c:925-950) for the next iteration, from the minimum gathered above
         double dt = bitsd(sc->dtmin_bits);
-        dt *= p.cfl;
+        dt *= cfl_at(p, sc->iter);
         if (p.tube && sc->t + dt > p.tmax) {
             dt = (p.tmax - sc->t);
             sc->stop_after = 1;

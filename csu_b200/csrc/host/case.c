@@ -334,6 +334,12 @@ static int setup(csu_case* cs, const char* mesh_text, size_t mesh_len, const cha
         c->sst_l = kw_dbl(kw, "Lsst", 1.0);
     }
     int restart = kw_int(kw, "restart", 0);
+    /* extensions */
+    c->implicit_fp32 = kw_int(kw, "implicitFP32", 0);
+    c->implicit_local_dt = kw_int(kw, "implicitLocalDt", 0);
+    c->cfl_ramp_iters = kw_int(kw, "CFLramp", 0);
+    c->cfl_max = kw_dbl(kw, "CFLmax", c->cfl);
+    c->conv_drop = kw_dbl(kw, "convDrop", 0.0);
 
     if (c->sa == 1 || c->sst == 1) csu_mesh_wall_distance(&cs->mesh);
 

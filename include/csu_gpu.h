@@ -77,6 +77,14 @@ typedef struct csu_config {
     double mach_inf;                      /* CONDITION.mach (AUSM+up M_inf)                       */
     double inlet_p, inlet_t;              /* CONDITION.p, CONDITION.T                             */
     double sst_l, k_factor, o_factor, o_wall_factor;
+    /* Extensions (no reference keyword semantics to follow; 0 keeps the reference behaviour). */
+    int implicit_fp32;       /* DPLUR blocks stored and applied in FP32 (keyword implicitFP32)           */
+    int implicit_local_dt;   /* implicit diagonal with each cell's own step, Omega/(CFL dtL_i)
+                                (keyword implicitLocalDt) instead of the global minimum step            */
+    int cfl_ramp_iters;      /* CFL grows geometrically from CFL to cfl_max over this many iterations
+                                (keywords CFLramp, CFLmax)                                              */
+    double cfl_max;
+    double conv_drop;        /* stop once res[0] <= conv_drop * res[0] of the first iteration (convDrop) */
 } csu_config;
 
 /*
@@ -158,6 +166,8 @@ int csu_residual(csu_ctx* ctx, double* R);
  * iteration counter of the first one (dtLocalN uses it). hist (nullable) gets n rows of
  * CSU_HIST_STRIDE(nvar) doubles. Returns CSU_ERR_NONFINITE if the state became non-finite. */
 int csu_iterate(csu_ctx* ctx, int n, int it0, double* hist);
+/* Same, also reporting how many iterations ran before the convergence stop (conv_drop) triggered. */
+int csu_iterate_ex(csu_ctx* ctx, int n, int it0, double* hist, int* n_done);
 
 /* The unsteady tube loop (solver.c:1912-1942) up to tmax; returns steps taken and final time. */
 int csu_tube_run(csu_ctx* ctx, double tmax, int* steps, double* t_final);
