@@ -75,6 +75,10 @@ class Clocks:
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # start timing only once the sampler runs (its start-up must not fall inside the timed region)
+            t0 = time.time()
+            while not self.samples and time.time() - t0 < 5.0:
+                time.sleep(0.01)
         except Exception:
             self.proc = None
         return self

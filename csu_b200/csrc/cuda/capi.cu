@@ -122,6 +122,7 @@ static void plan(csu_ctx* x, Arena& a)
     m.lm = carve<unsigned long long>(a, c4);
     m.les = carve<int>(a, c4);
     m.lrv = carve<unsigned long long>(a, nc);
+    m.lq = carve<double2>(a, c4);
     m.ex = carve<double>(a, c4);
     m.ey = carve<double>(a, c4);
     m.fslot = carve<int>(a, c4);
@@ -185,6 +186,7 @@ static void plan(csu_ctx* x, Arena& a)
     s.bcoef = carve<double>(a, (size_t)4 * (nb > 0 ? nb : 1));
     s.sc = carve<Scalars>(a, 1);
     s.dbg_ghost = carve<double>(a, (size_t)(nb > 0 ? nb : 1) * (nv + 1));
+    s.lsq_x87 = carve<unsigned long long>(a, 1);
 }
 
 static int upload_mesh(csu_ctx* x)
@@ -234,6 +236,7 @@ static int upload_mesh(csu_ctx* x)
     CK(up(m.lm, L.lm, sizeof(unsigned long long) * c4));
     CK(up(m.les, L.les, sizeof(int) * c4));
     CK(up(m.lrv, L.lrv, sizeof(unsigned long long) * nc));
+    CK(up(m.lq, L.lq, sizeof(double2) * c4));
     CK(up(m.ex, L.ex, sizeof(double) * c4));
     CK(up(m.ey, L.ey, sizeof(double) * c4));
     CK(up(m.fslot, L.fslot, sizeof(int) * c4));
@@ -325,8 +328,13 @@ static void fill_params(csu_ctx* x)
     p.o_wall_factor = c.o_wall_factor;
     p.tmax = 0;
     // exact x87 gradients unless CSU_LSQ_FAST=1 (FP64 weights: faster, last-bit differences)
+    // least squares: certified double-double with x87 fallback (default, bit-exact); CSU_LSQ=x87 runs the
+    // x87 model on every component; CSU_LSQ=weights (or CSU_LSQ_FAST=1) precomputed FP64 weights
     const char* fast = getenv("CSU_LSQ_FAST");
-    p.lsq_exact = (fast && fast[0] == '1') ? 0 : 1;
+    const char* lsq = getenv("CSU_LSQ");
+    p.lsq_exact = 2;
+    if (lsq && !strcmp(lsq, "x87")) p.lsq_exact = 1;
+    if ((lsq && !strcmp(lsq, "weights")) || (fast && fast[0] == '1')) p.lsq_exact = 0;
     p.visc = (c.laminar || c.sa || c.sst) ? 1 : 0;
     p.visc_blazek = c.visc_blazek;
     p.conv_tol = c.conv_drop;
@@ -444,6 +452,7 @@ extern "C" int csu_create(const csu_mesh_desc* md, const csu_config* cfg, csu_ct
         return st;
     }
     x->gb_c = (x->L.nc + BLOCK - 1) / BLOCK;
+
     x->gb_fi = (x->L.nf + BLOCK - 1) / BLOCK;
     x->gb_fb = (x->L.nb + BLOCK - 1) / BLOCK;
     switch (cfg->stages) {
@@ -523,11 +532,21 @@ extern "C" int csu_get_state_rows(csu_ctx* x, double* const* U)
 
 // ---------------------------------------------------------------------------------------------- launches
 
+template <int MODEL, bool DBG>
+static void launch_grad_lsq(csu_ctx* x)
+{
+    switch (x->prm.lsq_exact) {
+    case 0: k_grad<MODEL, DBG, 0><<<x->gb_c, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st); break;
+    case 1: k_grad<MODEL, DBG, 1><<<x->gb_c, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st); break;
+    default: k_grad<MODEL, DBG, 2><<<x->gb_c, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st); break;
+    }
+}
+
 template <int MODEL>
 static void launch_grad(csu_ctx* x, bool dbg)
 {
-    if (dbg) k_grad<MODEL, true><<<x->gb_c, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st);
-    else k_grad<MODEL, false><<<x->gb_c, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st);
+    if (dbg) launch_grad_lsq<MODEL, true>(x);
+    else launch_grad_lsq<MODEL, false>(x);
     x->launches++;
     tmark(x, KGRAD);
 }
@@ -912,6 +931,12 @@ extern "C" int csu_dump(csu_ctx* x, int what, double* out)
             for (int j = 0; j < 4; j++)
                 for (size_t e = 0; e < per; e++) o[j * per + e] = a[((size_t)j * per + e) * nc + c];
         }
+        return CSU_OK;
+    }
+    case CSU_DUMP_LSQ_X87: {
+        unsigned long long q = 0;
+        CK(cudaMemcpy(&q, x->st.lsq_x87, sizeof(q), cudaMemcpyDeviceToHost));
+        out[0] = (double)q;
         return CSU_OK;
     }
     default:

@@ -4,6 +4,7 @@
 #include <stdint.h>
 #include "physics.cuh"
 #include "ext80.cuh"
+#include "lsqdd.cuh"
 #include "viscous.cuh"
 #include "sa.cuh"
 #include "sst.cuh"
@@ -25,7 +26,8 @@ struct Prm {
     Gas gas;
     int nc, nf, nb;
     int order, scheme, laminar, sa, sst, axi, turb1order, limiter_type, stages, dt_local_n, tube, n_linear;
-    int lsq_exact;      // gradients with the reference's x87 rounding (1) or precomputed FP64 weights (0)
+    int lsq_exact;      // least squares: 0 precomputed FP64 weights (not bit-exact), 1 x87 model for every
+                        // component, 2 certified double-double + x87 model for the rest (bit-exact)
     int visc;           // laminar, SA or SST: temperature gradient and viscous fluxes
     int visc_blazek;    // SA face gradients with the directional correction (saInterFaceB)
     double lim_k, vol_max, e_fix, r_lim, p_out, t_wall, pr, pr_t, w_imp, cfl, sigma, mach_inf, sref;
@@ -77,6 +79,7 @@ struct Mesh {
     const unsigned long long* lm;   // [4][nc] x87 significands of a, b, c, det
     const int* les;                 // [4][nc] exponent << 1 | sign
     const unsigned long long* lrv;  // reciprocal of det's significand
+    const double2* lq;              // [4][nc] a, b, c and 1/det as exact (h, l) double-doubles
     const int* fslot;
     const double* omega;
     const double* sxh;
@@ -124,6 +127,7 @@ struct State {
     double* hist;                             // history rows
     Scalars* sc;
     double* dbg_ghost;                        // optional: ghost primitives [bface][NP] (reference order)
+    unsigned long long* lsq_x87;              // running count of gradient slots left to the integer x87 model
 };
 
 // ---------------------------------------------------------------- small helpers

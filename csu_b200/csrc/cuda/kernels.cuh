@@ -56,153 +56,292 @@ __global__ void __launch_bounds__(BLOCK) k_prim(const __grid_constant__ Prm p, c
 // ------------------------------------------------------------------------------------------------
 // k_grad: solverUpdateGrad + the limiter loop of inter (solver.c:451-548).
 // DBG also records ghost primitives (boundaryCalcPrimitive) in reference order.
+// LSQ selects the least-squares arithmetic (Prm::lsq_exact): 0 precomputed FP64 weights, 1 the integer x87
+// model (ext80.cuh) for every component, 2 the FP64 x87 emulation and certified double-double solve of
+// lsqdd.cuh, with the integer model only for the rare components those cannot decide (lsq_slot_x87).
 // ------------------------------------------------------------------------------------------------
-template <int MODEL, bool DBG>
-__global__ void __launch_bounds__(BLOCK) k_grad(const __grid_constant__ Prm p, const __grid_constant__ Mesh m,
-                                                const __grid_constant__ State s)
+
+// x87 constants a, b, c, det of cell c (solver.c:1063-1073, evaluated on the host in long double)
+__device__ __forceinline__ void lsq_consts(const Mesh& m, int nc, int c, X80* K)
 {
-    constexpr int NV = Model<MODEL>::NV, NP = Model<MODEL>::NP;
-    int c = blockIdx.x * BLOCK + threadIdx.x;
-    if (c >= m.nc || halted(s)) return;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        int es = m.les[(size_t)q * nc + c];
+        K[q].m = m.lm[(size_t)q * nc + c];
+        K[q].e = es >> 1;
+        K[q].s = es & 1;
+    }
+}
+
+// limiterCalc epsilon^2 of slot kk (limiter.c:98-119); aux = (K sqrt(omega / omega_max))^3 for type 0
+__device__ __forceinline__ double limiter_eps2(const Prm& p, const State& s, int kk, double aux)
+{
+    if (p.limiter_type == 0) return p.pref20[kk] * aux;
+    int mm = kk == 4 ? 5 : kk; // limiter.c:66-70 (SST reads k for both scalars)
+    int sl = mm > 4 ? mm - 1 : mm;
+    double a2 = (ordbits_inv(s.sc->qmax_bits[sl]) - ordbits_inv(s.sc->qmin_bits[sl])) * p.lim_k;
+    return a2 * a2;
+}
+
+// One gradient component pair of cell c for primitive vi (T: 4) with the integer x87 model, gathering the
+// neighbours again. Out of line: only the rare components the FP64 path cannot decide come here.
+template <int MODEL>
+__device__ __forceinline__ double2 lsq_slot_x87(const Prm& p, const Mesh& m, const State& s, int c, int vi)
+{
+    constexpr int NP = Model<MODEL>::NP;
     const int nc = m.nc;
     double P0[NP];
     loadP<MODEL>(s, nc, c, P0);
-    double gx[NV], gy[NV], qmin[NV], qmax[NV];
-    X80 XA[NV], XB[NV], TA = x80_zero(0), TB = x80_zero(0);
-    double gtx = 0.0, gty = 0.0;
-    const bool visc = p.visc != 0;
+    double u0 = 0.0;
 #pragma unroll
-    for (int kk = 0; kk < NV; kk++) {
-        gx[kk] = 0.0;
-        gy[kk] = 0.0;
-        qmin[kk] = P0[slot2p(kk)];
-        qmax[kk] = P0[slot2p(kk)];
-        XA[kk] = x80_zero(0);
-        XB[kk] = x80_zero(0);
-    }
-    const bool exact = p.lsq_exact != 0;
+    for (int k = 0; k < NP; k++)
+        if (k == vi) u0 = P0[k];
+    X80 XA = x80_zero(0), XB = x80_zero(0);
     const int np = m.npts[c];
     const double dw = m.wall_d ? m.wall_d[c] : 0.0;
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-        if (j < np) {
-            int n = m.nei[(size_t)j * nc + c];
-            double Pn[NP];
-            if (n < nc) {
-                loadP<MODEL>(s, nc, n, Pn);
-            } else {
-                int b = n - nc;
-                double2 dSv = m.bn[b];
-                ghost_state<MODEL>(p, m.bflag[b], dSv.x, dSv.y, m.bds[b], P0, dw, Pn);
-                if (DBG) {
-                    int bo = m.bold[b];
-                    for (int k = 0; k < NP; k++) s.dbg_ghost[(size_t)bo * NP + k] = Pn[k];
-                }
-            }
-            if (exact) {
-                // solverCalcGrad3 (solver.c:1063-1070): double products summed in long double
-                double dxj = m.ldx[(size_t)j * nc + c], dyj = m.ldy[(size_t)j * nc + c];
-                if (visc) {
-                    double dT = Pn[4] - P0[4];
-                    TA = x80_add(TA, x80_from_double(dxj * dT));
-                    TB = x80_add(TB, x80_from_double(dyj * dT));
-                }
-#pragma unroll
-                for (int kk = 0; kk < NV; kk++) {
-                    double du = Pn[slot2p(kk)] - P0[slot2p(kk)];
-                    XA[kk] = x80_add(XA[kk], x80_from_double(dxj * du));
-                    XB[kk] = x80_add(XB[kk], x80_from_double(dyj * du));
-                    qmax[kk] = fmax(qmax[kk], Pn[slot2p(kk)]);
-                    qmin[kk] = fmin(qmin[kk], Pn[slot2p(kk)]);
-                }
-            } else {
-                double wxj = m.wx[(size_t)j * nc + c], wyj = m.wy[(size_t)j * nc + c];
-                if (visc) {
-                    double dT = Pn[4] - P0[4];
-                    gtx += wxj * dT;
-                    gty += wyj * dT;
-                }
-#pragma unroll
-                for (int kk = 0; kk < NV; kk++) {
-                    double du = Pn[slot2p(kk)] - P0[slot2p(kk)];
-                    gx[kk] += wxj * du;
-                    gy[kk] += wyj * du;
-                    qmax[kk] = fmax(qmax[kk], Pn[slot2p(kk)]);
-                    qmin[kk] = fmin(qmin[kk], Pn[slot2p(kk)]);
-                }
-            }
+    for (int j = 0; j < np; j++) {
+        int n = m.nei[(size_t)j * nc + c];
+        double Pn[NP];
+        if (n < nc) {
+            loadP<MODEL>(s, nc, n, Pn);
+        } else {
+            int b = n - nc;
+            double2 dSv = m.bn[b];
+            ghost_state<MODEL>(p, m.bflag[b], dSv.x, dSv.y, m.bds[b], P0, dw, Pn);
         }
+        double un = 0.0;
+#pragma unroll
+        for (int k = 0; k < NP; k++)
+            if (k == vi) un = Pn[k];
+        double du = un - u0;
+        XA = x80_add(XA, x80_from_double(m.ldx[(size_t)j * nc + c] * du));
+        XB = x80_add(XB, x80_from_double(m.ldy[(size_t)j * nc + c] * du));
     }
-    if (exact) {
-        // dUx = (c A - b B) / (a c - b b), dUy = (-b A + a B) / (a c - b b) in long double (solver.c:1072-1073)
-        X80 K[4];
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-            int es = m.les[(size_t)q * nc + c];
-            K[q].m = m.lm[(size_t)q * nc + c];
-            K[q].e = es >> 1;
-            K[q].s = es & 1;
-        }
-        unsigned long long rv = m.lrv[c];
+    X80 K[4];
+    lsq_consts(m, nc, c, K);
+    unsigned long long rv = m.lrv[c];
+    X80 nx = x80_add(x80_mul(K[2], XA), x80_neg(x80_mul(K[1], XB)));
+    X80 ny = x80_add(x80_mul(x80_neg(K[1]), XA), x80_mul(K[0], XB));
+    atomicAdd(s.lsq_x87, 1ULL);
+    return make_double2(x80_to_double(x80_div_pre(nx, K[3], rv)), x80_to_double(x80_div_pre(ny, K[3], rv)));
+}
+
+template <int MODEL, bool DBG, int LSQ>
+__global__ void __launch_bounds__(BLOCK, 2) k_grad(const __grid_constant__ Prm p, const __grid_constant__ Mesh m,
+                                                const __grid_constant__ State s)
+{
+    constexpr int NV = Model<MODEL>::NV, NP = Model<MODEL>::NP;
+    const int c = blockIdx.x * BLOCK + threadIdx.x;
+    if (c >= m.nc || halted(s)) return;
+    {
+        const int nc = m.nc;
+        double P0[NP];
+        loadP<MODEL>(s, nc, c, P0);
+        double gx[NV], gy[NV], qmin[NV], qmax[NV];
+        X80 XA[NV], XB[NV], TA = x80_zero(0), TB = x80_zero(0);
+        DD AX[NV], AY[NV], TX = {0.0, 0.0}, TY = {0.0, 0.0};
+        bool sum_ok = true;
+        double gtx = 0.0, gty = 0.0;
+        const bool visc = p.visc != 0;
 #pragma unroll
         for (int kk = 0; kk < NV; kk++) {
-            X80 nx = x80_add(x80_mul(K[2], XA[kk]), x80_neg(x80_mul(K[1], XB[kk])));
-            X80 ny = x80_add(x80_mul(x80_neg(K[1]), XA[kk]), x80_mul(K[0], XB[kk]));
-            gx[kk] = x80_to_double(x80_div_pre(nx, K[3], rv));
-            gy[kk] = x80_to_double(x80_div_pre(ny, K[3], rv));
-        }
-        if (visc) {
-            // solverGrad_T (solver.c:477-490): the same least squares on T
-            X80 nx = x80_add(x80_mul(K[2], TA), x80_neg(x80_mul(K[1], TB)));
-            X80 ny = x80_add(x80_mul(x80_neg(K[1]), TA), x80_mul(K[0], TB));
-            gtx = x80_to_double(x80_div_pre(nx, K[3], rv));
-            gty = x80_to_double(x80_div_pre(ny, K[3], rv));
-        }
-    }
-    if (visc) {
-        s.GTx[c] = gtx;
-        s.GTy[c] = gty;
-    }
-    double phi[NV];
-#pragma unroll
-    for (int kk = 0; kk < NV; kk++) phi[kk] = 1.0;
-    if (p.order == 2) {
-        // limiterCalc (limiter.c:98-119), type 0: eps^2 = q_inf^2 (K sqrt(omega/omega_max))^3
-        double aux = p.lim_k * sqrt(m.omega[c] / p.vol_max);
-        aux = aux * aux * aux;
-        double ee[NV];
-#pragma unroll
-        for (int kk = 0; kk < NV; kk++) {
-            if (p.limiter_type == 0) {
-                ee[kk] = p.pref20[kk] * aux;
-            } else {
-                int mm = kk == 4 ? 5 : kk; // limiter.c:66-70 (SST reads k for both scalars)
-                int sl = mm > 4 ? mm - 1 : mm;
-                double a2 = (ordbits_inv(s.sc->qmax_bits[sl]) - ordbits_inv(s.sc->qmin_bits[sl])) * p.lim_k;
-                ee[kk] = a2 * a2;
+            gx[kk] = 0.0;
+            gy[kk] = 0.0;
+            qmin[kk] = P0[slot2p(kk)];
+            qmax[kk] = P0[slot2p(kk)];
+            if (LSQ == 1) {
+                XA[kk] = x80_zero(0);
+                XB[kk] = x80_zero(0);
+            }
+            if (LSQ == 2) {
+                AX[kk].h = AX[kk].l = 0.0;
+                AY[kk].h = AY[kk].l = 0.0;
             }
         }
-#pragma unroll
+        const int np = m.npts[c];
+        const double dw = m.wall_d ? m.wall_d[c] : 0.0;
+        // the FP64 path runs the neighbour loop rolled: one copy of the gather, ghost state and x87 steps
+        constexpr int JU = LSQ == 2 ? 1 : 4;
+#pragma unroll JU
         for (int j = 0; j < 4; j++) {
             if (j < np) {
-                double exj = m.ex[(size_t)j * nc + c], eyj = m.ey[(size_t)j * nc + c];
+                int n = m.nei[(size_t)j * nc + c];
+                double Pn[NP];
+                if (n < nc) {
+                    loadP<MODEL>(s, nc, n, Pn);
+                } else {
+                    int b = n - nc;
+                    double2 dSv = m.bn[b];
+                    ghost_state<MODEL>(p, m.bflag[b], dSv.x, dSv.y, m.bds[b], P0, dw, Pn);
+                    if (DBG) {
+                        int bo = m.bold[b];
+                        for (int k = 0; k < NP; k++) s.dbg_ghost[(size_t)bo * NP + k] = Pn[k];
+                    }
+                }
+                if (LSQ != 0) {
+                    // solverCalcGrad3 (solver.c:1063-1070): double products summed in long double
+                    double dxj = m.ldx[(size_t)j * nc + c], dyj = m.ldy[(size_t)j * nc + c];
+                    if (visc) {
+                        double dT = Pn[4] - P0[4];
+                        if (LSQ == 1) {
+                            TA = x80_add(TA, x80_from_double(dxj * dT));
+                            TB = x80_add(TB, x80_from_double(dyj * dT));
+                        } else if (j == 0) {
+                            TX.h = dxj * dT;
+                            TY.h = dyj * dT;
+                        } else if (j == 1) {
+                            TX = x87_sum2(TX.h, dxj * dT, sum_ok);
+                            TY = x87_sum2(TY.h, dyj * dT, sum_ok);
+                        } else {
+                            TX = x87_sum_add(TX, dxj * dT, sum_ok);
+                            TY = x87_sum_add(TY, dyj * dT, sum_ok);
+                        }
+                    }
 #pragma unroll
-                for (int kk = 0; kk < NV; kk++) {
-                    double d2 = (gx[kk] * exj + gy[kk] * eyj);
-                    double phi0 = limiterV2(P0[slot2p(kk)], qmin[kk], qmax[kk], d2, ee[kk]);
-                    phi[kk] = j == 0 ? phi0 : fmin(phi[kk], phi0);
+                    for (int kk = 0; kk < NV; kk++) {
+                        double du = Pn[slot2p(kk)] - P0[slot2p(kk)];
+                        if (LSQ == 1) {
+                            XA[kk] = x80_add(XA[kk], x80_from_double(dxj * du));
+                            XB[kk] = x80_add(XB[kk], x80_from_double(dyj * du));
+                        } else if (j == 0) {
+                            AX[kk].h = dxj * du;
+                            AY[kk].h = dyj * du;
+                        } else if (j == 1) {
+                            AX[kk] = x87_sum2(AX[kk].h, dxj * du, sum_ok);
+                            AY[kk] = x87_sum2(AY[kk].h, dyj * du, sum_ok);
+                        } else {
+                            AX[kk] = x87_sum_add(AX[kk], dxj * du, sum_ok);
+                            AY[kk] = x87_sum_add(AY[kk], dyj * du, sum_ok);
+                        }
+                        qmax[kk] = fmax(qmax[kk], Pn[slot2p(kk)]);
+                        qmin[kk] = fmin(qmin[kk], Pn[slot2p(kk)]);
+                    }
+                } else {
+                    double wxj = m.wx[(size_t)j * nc + c], wyj = m.wy[(size_t)j * nc + c];
+                    if (visc) {
+                        double dT = Pn[4] - P0[4];
+                        gtx += wxj * dT;
+                        gty += wyj * dT;
+                    }
+#pragma unroll
+                    for (int kk = 0; kk < NV; kk++) {
+                        double du = Pn[slot2p(kk)] - P0[slot2p(kk)];
+                        gx[kk] += wxj * du;
+                        gy[kk] += wyj * du;
+                        qmax[kk] = fmax(qmax[kk], Pn[slot2p(kk)]);
+                        qmin[kk] = fmin(qmin[kk], Pn[slot2p(kk)]);
+                    }
                 }
             }
         }
-    }
-    s.G4x[c] = make_double4(gx[0], gx[1], gx[2], gx[3]);
-    s.G4y[c] = make_double4(gy[0], gy[1], gy[2], gy[3]);
-    s.PH4[c] = make_double4(phi[0], phi[1], phi[2], phi[3]);
+        if (LSQ != 0) {
+            // dUx = (c A - b B) / (a c - b b), dUy = (-b A + a B) / (a c - b b) in long double (solver.c:1072-1073)
+            if (LSQ == 1) {
+                X80 K[4];
+                lsq_consts(m, nc, c, K);
+                unsigned long long rv = m.lrv[c];
 #pragma unroll
-    for (int kk = 4; kk < NV; kk++) {
-        s.Gxx[(size_t)(kk - 4) * nc + c] = gx[kk];
-        s.Gxy[(size_t)(kk - 4) * nc + c] = gy[kk];
-        s.PHx[(size_t)(kk - 4) * nc + c] = phi[kk];
+                for (int kk = 0; kk < NV; kk++) {
+                    X80 nx = x80_add(x80_mul(K[2], XA[kk]), x80_neg(x80_mul(K[1], XB[kk])));
+                    X80 ny = x80_add(x80_mul(x80_neg(K[1]), XA[kk]), x80_mul(K[0], XB[kk]));
+                    gx[kk] = x80_to_double(x80_div_pre(nx, K[3], rv));
+                    gy[kk] = x80_to_double(x80_div_pre(ny, K[3], rv));
+                }
+                if (visc) {
+                    // solverGrad_T (solver.c:477-490): the same least squares on T
+                    X80 nx = x80_add(x80_mul(K[2], TA), x80_neg(x80_mul(K[1], TB)));
+                    X80 ny = x80_add(x80_mul(x80_neg(K[1]), TA), x80_mul(K[0], TB));
+                    gtx = x80_to_double(x80_div_pre(nx, K[3], rv));
+                    gty = x80_to_double(x80_div_pre(ny, K[3], rv));
+                }
+            } else {
+                // a, b, c and 1/det as double-doubles, precomputed on the host
+                double2 qa = m.lq[c], qb = m.lq[(size_t)nc + c], qc = m.lq[(size_t)2 * nc + c];
+                double2 qr = m.lq[(size_t)3 * nc + c];
+                DD ka = {qa.x, qa.y}, kb = {qb.x, qb.y}, kc = {qc.x, qc.y}, R = {qr.x, qr.y};
+                // bit 2 kk + (0: x, 1: y) set where the cheap certified solve cannot decide; slot NV is T
+                unsigned need = 0;
+#pragma unroll
+                for (int kk = 0; kk < NV; kk++) {
+                    if (!lsq_certified(kc, kb, R, AX[kk], AY[kk], &gx[kk])) need |= 1u << (2 * kk);
+                    if (!lsq_certified(ka, kb, R, AY[kk], AX[kk], &gy[kk])) need |= 2u << (2 * kk);
+                }
+                if (visc) {
+                    if (!lsq_certified(kc, kb, R, TX, TY, &gtx)) need |= 1u << (2 * NV);
+                    if (!lsq_certified(ka, kb, R, TY, TX, &gty)) need |= 2u << (2 * NV);
+                }
+                if (!sum_ok) need = visc ? (4u << (2 * NV)) - 1u : (1u << (2 * NV)) - 1u;
+                // one out-of-loop copy of the exact-numerator solve, then of the integer x87 model
+#pragma unroll 1
+                while (need) {
+                    const int b = __ffs(need) - 1;
+                    need &= need - 1;
+                    const int kk = b >> 1, comp = b & 1;
+                    DD X = TX, Y = TY;
+#pragma unroll
+                    for (int q = 0; q < NV; q++) {
+                        if (q == kk) {
+                            X = AX[q];
+                            Y = AY[q];
+                        }
+                    }
+                    double g = 0.0;
+                    bool ok = sum_ok && (comp ? lsq_exact_numerator(ka, kb, R, Y, X, &g)
+                                              : lsq_exact_numerator(kc, kb, R, X, Y, &g));
+                    if (!ok) {
+                        double2 gg = lsq_slot_x87<MODEL>(p, m, s, c, kk < NV ? slot2p(kk) : 4);
+                        g = comp ? gg.y : gg.x;
+                    }
+                    if (kk == NV) {
+                        if (comp) gty = g;
+                        else gtx = g;
+                    }
+#pragma unroll
+                    for (int q = 0; q < NV; q++) {
+                        if (q == kk) {
+                            if (comp) gy[q] = g;
+                            else gx[q] = g;
+                        }
+                    }
+                }
+            }
+        }
+        if (visc) {
+            s.GTx[c] = gtx;
+            s.GTy[c] = gty;
+        }
+        double phi[NV];
+#pragma unroll
+        for (int kk = 0; kk < NV; kk++) phi[kk] = 1.0;
+        if (p.order == 2) {
+            // limiterCalc (limiter.c:98-119), type 0: eps^2 = q_inf^2 (K sqrt(omega/omega_max))^3
+            double aux = p.lim_k * sqrt(m.omega[c] / p.vol_max);
+            aux = aux * aux * aux;
+            double ee[NV];
+#pragma unroll
+            for (int kk = 0; kk < NV; kk++) ee[kk] = limiter_eps2(p, s, kk, aux);
+#pragma unroll JU
+            for (int j = 0; j < 4; j++) {
+                if (j < np) {
+                    double exj = m.ex[(size_t)j * nc + c], eyj = m.ey[(size_t)j * nc + c];
+#pragma unroll
+                    for (int kk = 0; kk < NV; kk++) {
+                        double d2 = (gx[kk] * exj + gy[kk] * eyj);
+                        double phi0 = limiterV2(P0[slot2p(kk)], qmin[kk], qmax[kk], d2, ee[kk]);
+                        phi[kk] = j == 0 ? phi0 : fmin(phi[kk], phi0);
+                    }
+                }
+            }
+        }
+        s.G4x[c] = make_double4(gx[0], gx[1], gx[2], gx[3]);
+        s.G4y[c] = make_double4(gy[0], gy[1], gy[2], gy[3]);
+        s.PH4[c] = make_double4(phi[0], phi[1], phi[2], phi[3]);
+#pragma unroll
+        for (int kk = 4; kk < NV; kk++) {
+            s.Gxx[(size_t)(kk - 4) * nc + c] = gx[kk];
+            s.Gxy[(size_t)(kk - 4) * nc + c] = gy[kk];
+            s.PHx[(size_t)(kk - 4) * nc + c] = phi[kk];
+        }
     }
 }
 

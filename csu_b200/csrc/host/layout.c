@@ -114,7 +114,7 @@ void csu_layout_free(csu_layout* L)
                     L->bface_old2new, L->npts, L->nint, L->nslot, L->nei, L->wx, L->wy, L->ex, L->ey,
                     L->fslot, L->omega, L->sxh, L->syh, L->xc, L->yc, L->wall_d, L->dslat, L->fe0, L->fe1,
                     L->fdsx, L->fdsy, L->fds, L->r0x, L->r0y, L->r1x, L->r1y, L->fdist, L->bown, L->bflag,
-                    L->bold, L->bdsx, L->bdsy, L->bds, L->bmx, L->bmy, L->ldx, L->ldy, L->lm, L->les, L->lrv,
+                    L->bold, L->bdsx, L->bdsy, L->bds, L->bmx, L->bmy, L->ldx, L->ldy, L->lm, L->les, L->lrv, L->lq,
                     L->fdx, L->fdy, L->bdx, L->bdy, L->bL, L->bunx, L->buny, L->bds2, L->color,
                     L->color_start, L->color_cells};
     for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); i++) free(ptrs[i]);
@@ -135,7 +135,7 @@ int csu_layout_build(const csu_mesh_desc* m, int axi, csu_layout* L)
     ALLOC(L->bface_new2old, nb); ALLOC(L->bface_old2new, nb);
     ALLOC(L->npts, nc); ALLOC(L->nint, nc); ALLOC(L->nslot, nc); ALLOC(L->nei, c4);
     ALLOC(L->wx, c4); ALLOC(L->wy, c4); ALLOC(L->ex, c4); ALLOC(L->ey, c4); ALLOC(L->fslot, c4);
-    ALLOC(L->ldx, c4); ALLOC(L->ldy, c4); ALLOC(L->lm, c4); ALLOC(L->les, c4); ALLOC(L->lrv, nc);
+    ALLOC(L->ldx, c4); ALLOC(L->ldy, c4); ALLOC(L->lm, c4); ALLOC(L->les, c4); ALLOC(L->lrv, nc); ALLOC(L->lq, 2 * c4);
     ALLOC(L->omega, nc); ALLOC(L->sxh, nc); ALLOC(L->syh, nc); ALLOC(L->xc, nc); ALLOC(L->yc, nc);
     ALLOC(L->dslat, nc);
     if (m->wall_dist) ALLOC(L->wall_d, nc);
@@ -326,6 +326,22 @@ int csu_layout_build(const csu_mesh_desc* m, int axi, csu_layout* L)
         long double k4[4] = {a, bb, cc, det};
         for (int q = 0; q < 4; q++) split_ld(k4[q], &L->lm[(size_t)q * nc + c], &L->les[(size_t)q * nc + c]);
         L->lrv[c] = recip64(L->lm[(size_t)3 * nc + c]);
+        /* the same as exact double-doubles for the device's certified FP64 evaluation: a, b, c as
+           (RN53, remainder) and 1/det to ~2^-103 (FP64 reciprocal + one Newton correction) */
+        for (int q = 0; q < 3; q++) {
+            double h = (double)k4[q];
+            L->lq[2 * ((size_t)q * nc + c)] = h;
+            L->lq[2 * ((size_t)q * nc + c) + 1] = (double)(k4[q] - (long double)h);
+        }
+        {
+            double dh = (double)det, dl = (double)(det - (long double)dh);
+            double r = 1.0 / dh;
+            double e = fma(-dh, r, 1.0);
+            e = e - dl * r;
+            double re = e * r, rs = r + re;
+            L->lq[2 * ((size_t)3 * nc + c)] = rs;
+            L->lq[2 * ((size_t)3 * nc + c) + 1] = re - (rs - r);
+        }
         for (int j = 0; j < np; j++) {
             L->ldx[(size_t)j * nc + c] = dx[j];
             L->ldy[(size_t)j * nc + c] = dy[j];

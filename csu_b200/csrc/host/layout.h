@@ -35,6 +35,7 @@ typedef struct csu_layout {
     unsigned long long* lm;  /* [4][nc] x87 significands of a, b, c, a*c - b*b (long double, solver.c:1058-1073) */
     int* les;      /* [4][nc] exponent << 1 | sign of the same                                          */
     unsigned long long* lrv; /* [nc] invariant-divisor reciprocal of the determinant's significand       */
+    double* lq;    /* [4][nc][2] a, b, c, 1/(a*c - b*b) as (high, low) double pairs                          */
     double* ex;    /* [4][nc] edge midpoint minus centroid, edges in node order (limiter, inter)        */
     double* ey;
     int* fslot;    /* [4][nc] +-(flux index + 1): interior faces (ELEMENT.f order) then boundary faces  */

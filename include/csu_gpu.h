@@ -182,7 +182,10 @@ int csu_tube_run(csu_ctx* ctx, double tmax, int* steps, double* t_final);
  *  CSU_DUMP_D       ncells                      implicit diagonal D (after an implicit iteration)
  *  CSU_DUMP_DTL     ncells                      dtL (local steps, or Omega/Lc for implicit)
  *  CSU_DUMP_DW      nvar*ncells                 last implicit increment dW1
- *  CSU_DUMP_BLOCKS  ncells*4*nvar*nvar          DPLUR blocks [cell][slot][row][col], slots in ELEMENT.f order */
+ *  CSU_DUMP_BLOCKS  ncells*4*nvar*nvar          DPLUR blocks [cell][slot][row][col], slots in ELEMENT.f order
+ *  CSU_DUMP_LSQ_X87 1                           gradient slots (cell, variable) so far that the FP64
+ *                                               least squares could not decide and left to the integer x87
+ *                                               model (no reference counterpart: a diagnostic of this engine) */
 #define CSU_DUMP_P 1
 #define CSU_DUMP_GHOST_P 2
 #define CSU_DUMP_GRAD 3
@@ -193,6 +196,7 @@ int csu_tube_run(csu_ctx* ctx, double tmax, int* steps, double* t_final);
 #define CSU_DUMP_DTL 8
 #define CSU_DUMP_DW 9
 #define CSU_DUMP_BLOCKS 10
+#define CSU_DUMP_LSQ_X87 11
 int csu_dump(csu_ctx* ctx, int what, double* out);
 
 /* Run the engine's work on a caller-provided cudaStream_t (NULL: the context's own stream). */

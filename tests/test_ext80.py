@@ -17,3 +17,19 @@ def test_ext80_matches_x87(tmp_path):
     r = subprocess.run([exe, "400000"], capture_output=True, text=True)
     assert r.returncode == 0, r.stdout + r.stderr
     assert "add=0 mul=0 div=0 cvt=0 grad=0" in r.stdout
+
+
+@pytest.mark.skipif(platform.machine() != "x86_64", reason="needs x87 long double")
+def test_certified_double_double_matches_x87(tmp_path):
+    """lsqdd.cuh: the FP64 emulation of single x87 operations (accumulation step, product, sum) equals the
+    host's x87 results on random, tie-prone, power-of-two and cancelling operands, and every gradient
+    component the certified and exact-numerator solves return equals the x87 formula (random cells plus
+    near-cancelling, one-directional, near-uniform and uniform fields); over 99 % of components decide."""
+    exe = str(tmp_path / "lsqdd_check")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-o", exe,
+                    os.path.join(ROOT, "tests", "native", "lsqdd_check.cpp")], check=True)
+    r = subprocess.run([exe, "1000000"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    f = dict(kv.split("=") for kv in r.stdout.replace("|", " ").split() if "=" in kv)
+    assert f["op_mismatches"] == "0" and f["mismatches"] == "0" and f["sum_mismatches"] == "0", r.stdout
+    assert float(f["certified"]) + float(f["exact_numerator"]) > 0.99, r.stdout
