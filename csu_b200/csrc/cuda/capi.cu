@@ -35,7 +35,11 @@ struct csu_ctx {
     int model = 0, nv = 4;
     csu_config cfg;
     csu_layout L;
-    Prm prm;
+    Prm prm;                 // parameters of solve 0 (the only one outside packs)
+    int nsolve = 1;
+    std::vector<Prm> prms;   // per solve, mirrored at d_prm
+    Prm* d_prm = nullptr;
+    double* hist = nullptr;  // nsolve blocks of hist_cap rows
     Mesh mesh;
     State st;
     Arena arena;
@@ -184,7 +188,8 @@ static void plan(csu_ctx* x, Arena& a)
     s.blocks32 = dplur && x->cfg.implicit_fp32 ? carve<float>(a, c4 * nv * nv) : nullptr;
     s.part = carve<double>(a, (size_t)((nc + BLOCK - 1) / BLOCK) * nv);
     s.bcoef = carve<double>(a, (size_t)4 * (nb > 0 ? nb : 1));
-    s.sc = carve<Scalars>(a, 1);
+    s.sc = carve<Scalars>(a, x->nsolve);
+    x->d_prm = carve<Prm>(a, x->nsolve);
     s.dbg_ghost = carve<double>(a, (size_t)(nb > 0 ? nb : 1) * (nv + 1));
     s.lsq_x87 = carve<unsigned long long>(a, 1);
 }
@@ -344,21 +349,53 @@ static void fill_params(csu_ctx* x)
     p.cfl_max = c.cfl_ramp_iters > 0 ? c.cfl_max : c.cfl;
 }
 
+static double* hist_of(csu_ctx* x, int k)
+{
+    return x->hist ? x->hist + (size_t)k * x->hist_cap * (x->nv + 4) : nullptr;
+}
+
 static int reset_scalars(csu_ctx* x, int it0)
 {
-    Scalars h;
-    memset(&h, 0, sizeof(h));
-    h.dtmin_bits = 0x7ff0000000000000ULL;
-    h.dt_local = x->cfg.dt_local;
-    h.iter = it0;
-    CK(cudaMemcpyAsync(x->st.sc, &h, sizeof(h), cudaMemcpyHostToDevice, x->stream));
+    std::vector<Scalars> hs(x->nsolve);
+    for (int k = 0; k < x->nsolve; k++) {
+        Scalars& h = hs[k];
+        memset(&h, 0, sizeof(h));
+        h.dtmin_bits = 0x7ff0000000000000ULL;
+        h.dt_local = x->cfg.dt_local;
+        h.iter = it0;
+        h.hist = hist_of(x, k);
+        h.hist_cap = x->hist_cap;
+    }
+    CK(cudaStreamSynchronize(x->stream));
+    CK(cudaMemcpy(x->st.sc, hs.data(), sizeof(Scalars) * hs.size(), cudaMemcpyHostToDevice));
+    return CSU_OK;
+}
+
+// scalars of solves [0, n)
+static int read_scalars_n(csu_ctx* x, Scalars* h, int n)
+{
+    CK(cudaStreamSynchronize(x->stream));
+    CK(cudaMemcpy(h, x->st.sc, sizeof(Scalars) * n, cudaMemcpyDeviceToHost));
     return CSU_OK;
 }
 
 static int read_scalars(csu_ctx* x, Scalars* h)
 {
-    CK(cudaMemcpyAsync(h, x->st.sc, sizeof(Scalars), cudaMemcpyDeviceToHost, x->stream));
+    return read_scalars_n(x, h, 1);
+}
+
+static int write_scalars_n(csu_ctx* x, const Scalars* h, int n)
+{
     CK(cudaStreamSynchronize(x->stream));
+    CK(cudaMemcpy(x->st.sc, h, sizeof(Scalars) * n, cudaMemcpyHostToDevice));
+    return CSU_OK;
+}
+
+// host parameters to the device copy (after any change of prms)
+static int upload_prm(csu_ctx* x)
+{
+    CK(cudaStreamSynchronize(x->stream));
+    CK(cudaMemcpy(x->d_prm, x->prms.data(), sizeof(Prm) * x->nsolve, cudaMemcpyHostToDevice));
     return CSU_OK;
 }
 
@@ -447,11 +484,21 @@ extern "C" int csu_create(const csu_mesh_desc* md, const csu_config* cfg, csu_ct
         delete x;
         return cuda_fail(e, "context setup");
     }
-    if ((st = upload_mesh(x)) || (st = reset_scalars(x, 0))) {
+    x->gb_c = (x->L.nc + BLOCK - 1) / BLOCK;
+    if ((st = upload_mesh(x))) {
         csu_destroy(x);
         return st;
     }
-    x->gb_c = (x->L.nc + BLOCK - 1) / BLOCK;
+    x->prm.cell0 = 0;
+    x->prm.blk0 = 0;
+    x->prm.nblk = x->gb_c;
+    x->prm.wall0 = 0;
+    x->prm.nwall = x->nwall;
+    x->prms.assign(1, x->prm);
+    if ((st = upload_prm(x)) || (st = reset_scalars(x, 0))) {
+        csu_destroy(x);
+        return st;
+    }
 
     x->gb_fi = (x->L.nf + BLOCK - 1) / BLOCK;
     x->gb_fb = (x->L.nb + BLOCK - 1) / BLOCK;
@@ -469,7 +516,7 @@ extern "C" void csu_destroy(csu_ctx* x)
 {
     if (!x) return;
     if (x->graph) cudaGraphExecDestroy(x->graph);
-    if (x->st.hist) cudaFree(x->st.hist);
+    if (x->hist) cudaFree(x->hist);
     for (cudaEvent_t e : x->ev) cudaEventDestroy(e);
     if (x->own_stream) cudaStreamDestroy(x->own_stream);
     if (x->arena.base) cudaFree(x->arena.base);
@@ -536,9 +583,9 @@ template <int MODEL, bool DBG>
 static void launch_grad_lsq(csu_ctx* x)
 {
     switch (x->prm.lsq_exact) {
-    case 0: k_grad<MODEL, DBG, 0><<<x->gb_c, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st); break;
-    case 1: k_grad<MODEL, DBG, 1><<<x->gb_c, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st); break;
-    default: k_grad<MODEL, DBG, 2><<<x->gb_c, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st); break;
+    case 0: k_grad<MODEL, DBG, 0><<<x->gb_c, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st); break;
+    case 1: k_grad<MODEL, DBG, 1><<<x->gb_c, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st); break;
+    default: k_grad<MODEL, DBG, 2><<<x->gb_c, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st); break;
     }
 }
 
@@ -554,7 +601,7 @@ static void launch_grad(csu_ctx* x, bool dbg)
 template <int MODEL>
 static void launch_flux(csu_ctx* x, int coef)
 {
-    k_flux<MODEL><<<x->gb_fi + x->gb_fb, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st, x->gb_fi, x->d_wall_rank,
+    k_flux<MODEL><<<x->gb_fi + x->gb_fb, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st, x->gb_fi, x->d_wall_rank,
                                                                  coef);
     x->launches++;
     tmark(x, KFLUX);
@@ -563,7 +610,7 @@ static void launch_flux(csu_ctx* x, int coef)
 template <int MODEL>
 static void launch_finalize(csu_ctx* x, int mode)
 {
-    k_finalize<MODEL><<<1, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st, x->gb_c, x->nwall, mode, x->hist_cap);
+    k_finalize<MODEL><<<x->nsolve, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st, mode);
     x->launches++;
     tmark(x, KFIN);
 }
@@ -572,7 +619,7 @@ template <int MODEL>
 static void launch_prologue(csu_ctx* x)
 {
     int rk = x->cfg.time_scheme == CSU_TS_RK;
-    k_prim<MODEL><<<x->gb_c, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st, rk);
+    k_prim<MODEL><<<x->gb_c, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st, rk);
     x->launches++;
     tmark(x, KPRIM);
     launch_finalize<MODEL>(x, 2);
@@ -588,8 +635,8 @@ static void launch_iteration(csu_ctx* x)
             bool last = sgi == c.stages - 1;
             if (c.order == 2 || x->prm.visc) launch_grad<MODEL>(x, false);
             launch_flux<MODEL>(x, last ? 1 : 0);
-            if (last) k_rk<MODEL, true><<<x->gb_c, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st, x->rk[sgi]);
-            else k_rk<MODEL, false><<<x->gb_c, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st, x->rk[sgi]);
+            if (last) k_rk<MODEL, true><<<x->gb_c, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st, x->rk[sgi]);
+            else k_rk<MODEL, false><<<x->gb_c, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st, x->rk[sgi]);
             x->launches++;
             tmark(x, KRK);
         }
@@ -597,7 +644,7 @@ static void launch_iteration(csu_ctx* x)
     } else if (c.time_scheme == CSU_TS_LUSGS) {
         if (c.order == 2 || x->prm.visc) launch_grad<MODEL>(x, false);
         launch_flux<MODEL>(x, 1);
-        k_impl<MODEL, false><<<x->gb_c, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st);
+        k_impl<MODEL, false><<<x->gb_c, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st);
         x->launches++;
         tmark(x, KIMPL);
         const int K = x->L.ncolors;
@@ -608,28 +655,28 @@ static void launch_iteration(csu_ctx* x)
                 if (count == 0) continue;
                 int g = (count + BLOCK - 1) / BLOCK;
                 if (pass == 0)
-                    k_lusgs<MODEL, true><<<g, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st, x->mesh.color,
+                    k_lusgs<MODEL, true><<<g, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st, x->mesh.color,
                                                                      x->mesh.color_cells, col, start, count);
                 else
-                    k_lusgs<MODEL, false><<<g, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st, x->mesh.color,
+                    k_lusgs<MODEL, false><<<g, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st, x->mesh.color,
                                                                       x->mesh.color_cells, col, start, count);
                 x->launches++;
                 tmark(x, KSWEEP);
             }
-        k_update<MODEL><<<x->gb_c, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st);
+        k_update<MODEL><<<x->gb_c, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st);
         x->launches++;
         tmark(x, KPRIM);
         launch_finalize<MODEL>(x, 1);
     } else {
         if (c.order == 2 || x->prm.visc) launch_grad<MODEL>(x, false);
         launch_flux<MODEL>(x, 1);
-        k_impl<MODEL, true><<<x->gb_c, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st);
+        k_impl<MODEL, true><<<x->gb_c, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st);
         x->launches++;
         tmark(x, KIMPL);
         for (int m = 0; m < c.n_linear; m++) {
             if (m == c.n_linear - 1)
-                k_sweep<MODEL, true><<<x->gb_c, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st, m, x->xcur);
-            else k_sweep<MODEL, false><<<x->gb_c, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st, m, x->xcur);
+                k_sweep<MODEL, true><<<x->gb_c, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st, m, x->xcur);
+            else k_sweep<MODEL, false><<<x->gb_c, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st, m, x->xcur);
             x->launches++;
             tmark(x, KSWEEP);
             x->xcur ^= 1;
@@ -641,11 +688,11 @@ static void launch_iteration(csu_ctx* x)
 template <int MODEL>
 static void launch_residual(csu_ctx* x, bool dbg)
 {
-    k_prim<MODEL><<<x->gb_c, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st, 0);
+    k_prim<MODEL><<<x->gb_c, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st, 0);
     x->launches++;
     if (x->cfg.order == 2 || dbg) launch_grad<MODEL>(x, dbg);
     launch_flux<MODEL>(x, 1);
-    k_resid<MODEL><<<x->gb_c, BLOCK, 0, x->stream>>>(x->prm, x->mesh, x->st);
+    k_resid<MODEL><<<x->gb_c, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st);
     x->launches++;
     launch_finalize<MODEL>(x, 3);
 }
@@ -670,10 +717,20 @@ static int ensure_hist(csu_ctx* x, int n)
 {
     if (n <= x->hist_cap) return CSU_OK;
     int cap = n < 1024 ? 1024 : n;
-    if (x->st.hist) CK(cudaFree(x->st.hist));
-    x->st.hist = nullptr;
-    CK(cudaMalloc((void**)&x->st.hist, sizeof(double) * (size_t)cap * (x->nv + 4)));
+    CK(cudaStreamSynchronize(x->stream));
+    if (x->hist) CK(cudaFree(x->hist));
+    x->hist = nullptr;
+    CK(cudaMalloc((void**)&x->hist, sizeof(double) * (size_t)cap * (x->nv + 4) * x->nsolve));
     x->hist_cap = cap;
+    // point every solve's scalars at its new rows
+    std::vector<Scalars> hs(x->nsolve);
+    int st;
+    if ((st = read_scalars_n(x, hs.data(), x->nsolve))) return st;
+    for (int k = 0; k < x->nsolve; k++) {
+        hs[k].hist = hist_of(x, k);
+        hs[k].hist_cap = cap;
+    }
+    if ((st = write_scalars_n(x, hs.data(), x->nsolve))) return st;
     if (x->graph) {
         cudaGraphExecDestroy(x->graph);
         x->graph = nullptr;
@@ -716,12 +773,14 @@ static int run_iterations(csu_ctx* x, int n, int it0, Scalars* out)
         x->prepared = 1;
     } else {
         // keep the device step state, restart the history rows and the loop counter
-        Scalars h;
-        if ((st = read_scalars(x, &h))) return st;
-        h.hist_row = 0;
-        h.iter = it0;
-        h.steps = 0;
-        CK(cudaMemcpyAsync(x->st.sc, &h, sizeof(h), cudaMemcpyHostToDevice, x->stream));
+        std::vector<Scalars> hs(x->nsolve);
+        if ((st = read_scalars_n(x, hs.data(), x->nsolve))) return st;
+        for (Scalars& h : hs) {
+            h.hist_row = 0;
+            h.iter = it0;
+            h.steps = 0;
+        }
+        if ((st = write_scalars_n(x, hs.data(), x->nsolve))) return st;
     }
     // graphs of G iterations; G even so the DPLUR increment buffers come back to the same parity
     const int G = 8;
@@ -752,7 +811,7 @@ extern "C" int csu_iterate_ex(csu_ctx* x, int n, int it0, double* hist, int* n_d
     if (st) return st;
     if (hist) {
         int rows = h.hist_row < n ? h.hist_row : n;
-        CK(cudaMemcpy(hist, x->st.hist, sizeof(double) * (size_t)rows * (x->nv + 4), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpy(hist, x->hist, sizeof(double) * (size_t)rows * (x->nv + 4), cudaMemcpyDeviceToHost));
     }
     if (h.status) {
         csu_set_error("csu_iterate: state became non-finite at iteration %d", h.iter);
@@ -774,6 +833,10 @@ extern "C" int csu_tube_run(csu_ctx* x, double tmax, int* steps, double* t_final
     }
     x->prm.tube = 1;
     x->prm.tmax = tmax;
+    x->prms[0].tube = 1;
+    x->prms[0].tmax = tmax;
+    int st0 = upload_prm(x);
+    if (st0) return st0;
     x->prepared = 0;
     if (x->graph) {
         cudaGraphExecDestroy(x->graph);
@@ -810,7 +873,7 @@ extern "C" int csu_residual(csu_ctx* x, double* R)
     if ((st = read_scalars(x, &h))) return st;
     h.done = 0;
     h.status = 0;
-    CK(cudaMemcpyAsync(x->st.sc, &h, sizeof(h), cudaMemcpyHostToDevice, x->stream));
+    if ((st = write_scalars_n(x, &h, 1))) return st;
     DISPATCH(launch_residual, x, true);
     if ((st = check_launch("residual"))) return st;
     x->prepared = 0;

@@ -38,6 +38,9 @@ struct Prm {
     SstK sst_k;         // SST constants (sstInit)
     double tmax;        // tube end time
     double conv_tol;    // stop when res[0] <= conv_tol * res0[0] (0: never)
+    int cell0;          // first cell of this solve (packs: cells [cell0, cell0 + nc), block aligned)
+    int blk0, nblk;     // its cell blocks (residual-norm partial sums)
+    int wall0, nwall;   // its wall faces in the wall-coefficient array
     int blk32;          // DPLUR blocks in FP32
     int implicit_local_dt;
     int cfl_ramp_iters; // CFL ramp (0: constant CFL)
@@ -62,6 +65,8 @@ struct Scalars {
     int hist_row;                         // next history row
     int steps;                            // iterations completed in this call
     int have_res0;                        // res0 recorded
+    int hist_cap;                         // rows available at hist
+    double* hist;                         // history rows of this solve (or null)
 };
 
 struct Mesh {
@@ -124,8 +129,9 @@ struct State {
     float* blocks32;                          // the same in FP32 (mixed-precision DPLUR)
     double* part;                             // per-block partial sums of R^2 [block][NV]
     double* bcoef;                            // per reference boundary face: cp dSx, cp dSy, fx/q, fy/q
-    double* hist;                             // history rows
-    Scalars* sc;
+    Scalars* sc;                              // one per solve
+    const int* bsolve;                        // packs: solve of each cell block (null: one solve)
+    const int* csolve;                        // packs: solve of each cell (null: one solve)
     double* dbg_ghost;                        // optional: ghost primitives [bface][NP] (reference order)
     unsigned long long* lsq_x87;              // running count of gradient slots left to the integer x87 model
 };

@@ -19,9 +19,26 @@
 
 namespace csu {
 
-__device__ __forceinline__ bool halted(const State& s)
+__device__ __forceinline__ bool halted(const Scalars* sc)
 {
-    return (s.sc->status | s.sc->done) != 0;
+    return (sc->status | sc->done) != 0;
+}
+
+// Solve of a cell block (in a pack every block holds cells of one solve) and of a cell; cells of the
+// solve are [p.cell0, p.cell0 + p.nc), the rest of its last block is padding.
+__device__ __forceinline__ int block_solve(const State& s)
+{
+    return s.bsolve ? s.bsolve[blockIdx.x] : 0;
+}
+
+__device__ __forceinline__ int cell_solve(const State& s, int c)
+{
+    return s.csolve ? s.csolve[c] : 0;
+}
+
+__device__ __forceinline__ bool cell_in(const Prm& p, int c)
+{
+    return (unsigned)(c - p.cell0) < (unsigned)p.nc;
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -29,18 +46,21 @@ __device__ __forceinline__ bool halted(const State& s)
 // step of the unclamped state first (solverCalcDt precedes solverCalcR, solver.c:1868-1869).
 // ------------------------------------------------------------------------------------------------
 template <int MODEL>
-__global__ void __launch_bounds__(BLOCK) k_prim(const __grid_constant__ Prm p, const __grid_constant__ Mesh m,
+__global__ void __launch_bounds__(BLOCK) k_prim(const Prm* __restrict__ P, const __grid_constant__ Mesh m,
                                                 const __grid_constant__ State s, int with_dt)
 {
     constexpr int NV = Model<MODEL>::NV, NP = Model<MODEL>::NP;
+    const int sid = block_solve(s);
+    const Prm& p = P[sid];
+    Scalars* const sc = s.sc + sid;
     int c = blockIdx.x * BLOCK + threadIdx.x;
     double lmin = __longlong_as_double(0x7ff0000000000000LL);
-    if (c < m.nc) {
+    if (cell_in(p, c)) {
         double U[NV], P[NP];
         loadU<MODEL>(s, m.nc, c, U);
         if (with_dt) {
             double l = local_step<MODEL>(p, U, m.sxh[c], m.syh[c], m.omega[c]);
-            s.dtl[c] = cfl_at(p, s.sc->iter) * l;
+            s.dtl[c] = cfl_at(p, sc->iter) * l;
             lmin = l;
         }
         clamp_prim<MODEL>(p, U, P);
@@ -49,7 +69,7 @@ __global__ void __launch_bounds__(BLOCK) k_prim(const __grid_constant__ Prm p, c
     }
     if (with_dt) {
         double v = warp_min(lmin);
-        if ((threadIdx.x & 31) == 0 && !(v > bitsd(0x7fefffffffffffffULL))) atomicMin(&s.sc->dtmin_bits, dbits(v));
+        if ((threadIdx.x & 31) == 0 && !(v > bitsd(0x7fefffffffffffffULL))) atomicMin(&sc->dtmin_bits, dbits(v));
     }
 }
 
@@ -74,12 +94,12 @@ __device__ __forceinline__ void lsq_consts(const Mesh& m, int nc, int c, X80* K)
 }
 
 // limiterCalc epsilon^2 of slot kk (limiter.c:98-119); aux = (K sqrt(omega / omega_max))^3 for type 0
-__device__ __forceinline__ double limiter_eps2(const Prm& p, const State& s, int kk, double aux)
+__device__ __forceinline__ double limiter_eps2(const Prm& p, const Scalars* sc, int kk, double aux)
 {
     if (p.limiter_type == 0) return p.pref20[kk] * aux;
     int mm = kk == 4 ? 5 : kk; // limiter.c:66-70 (SST reads k for both scalars)
     int sl = mm > 4 ? mm - 1 : mm;
-    double a2 = (ordbits_inv(s.sc->qmax_bits[sl]) - ordbits_inv(s.sc->qmin_bits[sl])) * p.lim_k;
+    double a2 = (ordbits_inv(sc->qmax_bits[sl]) - ordbits_inv(sc->qmin_bits[sl])) * p.lim_k;
     return a2 * a2;
 }
 
@@ -127,12 +147,15 @@ __device__ __forceinline__ double2 lsq_slot_x87(const Prm& p, const Mesh& m, con
 }
 
 template <int MODEL, bool DBG, int LSQ>
-__global__ void __launch_bounds__(BLOCK, 2) k_grad(const __grid_constant__ Prm p, const __grid_constant__ Mesh m,
+__global__ void __launch_bounds__(BLOCK, 2) k_grad(const Prm* __restrict__ P, const __grid_constant__ Mesh m,
                                                 const __grid_constant__ State s)
 {
     constexpr int NV = Model<MODEL>::NV, NP = Model<MODEL>::NP;
+    const int sid = block_solve(s);
+    const Prm& p = P[sid];
+    Scalars* const sc = s.sc + sid;
     const int c = blockIdx.x * BLOCK + threadIdx.x;
-    if (c >= m.nc || halted(s)) return;
+    if (!cell_in(p, c) || halted(sc)) return;
     {
         const int nc = m.nc;
         double P0[NP];
@@ -319,7 +342,7 @@ __global__ void __launch_bounds__(BLOCK, 2) k_grad(const __grid_constant__ Prm p
             aux = aux * aux * aux;
             double ee[NV];
 #pragma unroll
-            for (int kk = 0; kk < NV; kk++) ee[kk] = limiter_eps2(p, s, kk, aux);
+            for (int kk = 0; kk < NV; kk++) ee[kk] = limiter_eps2(p, sc, kk, aux);
 #pragma unroll JU
             for (int j = 0; j < 4; j++) {
                 if (j < np) {
@@ -350,17 +373,19 @@ __global__ void __launch_bounds__(BLOCK, 2) k_grad(const __grid_constant__ Prm p
 // coef: also record the wall pressure-coefficient terms of solverCalcCoeff3 (solver.c:1360-1385).
 // ------------------------------------------------------------------------------------------------
 template <int MODEL>
-__global__ void __launch_bounds__(BLOCK) k_flux(const __grid_constant__ Prm p, const __grid_constant__ Mesh m,
+__global__ void __launch_bounds__(BLOCK) k_flux(const Prm* __restrict__ P, const __grid_constant__ Mesh m,
                                                 const __grid_constant__ State s, int nbi, const int* wall_rank,
                                                 int coef)
 {
     constexpr int NV = Model<MODEL>::NV, NP = Model<MODEL>::NP;
-    if (halted(s)) return;
     const int nc = m.nc;
     if ((int)blockIdx.x < nbi) {
         int f = blockIdx.x * BLOCK + threadIdx.x;
         if (f >= m.nf) return;
         int2 e = m.fe[f];
+        const int sid = cell_solve(s, e.x);
+        const Prm& p = P[sid];
+        if (halted(s.sc + sid)) return;
         double2 dSv = m.fn[f];
         double dSx = dSv.x, dSy = dSv.y, dS = m.fds[f];
         double PL[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
@@ -442,6 +467,9 @@ __global__ void __launch_bounds__(BLOCK) k_flux(const __grid_constant__ Prm p, c
         int b = (blockIdx.x - nbi) * BLOCK + threadIdx.x;
         if (b >= m.nb) return;
         int c = m.bown[b];
+        const int sid = cell_solve(s, c);
+        const Prm& p = P[sid];
+        if (halted(s.sc + sid)) return;
         int flag = m.bflag[b];
         double2 dSv = m.bn[b];
         double dSx = dSv.x, dSy = dSv.y, dS = m.bds[b];
@@ -625,17 +653,18 @@ __device__ __forceinline__ void partial_norms(const State& s, bool valid, const 
 // k_resid: R only (csu_residual).
 // ------------------------------------------------------------------------------------------------
 template <int MODEL>
-__global__ void __launch_bounds__(BLOCK) k_resid(const __grid_constant__ Prm p, const __grid_constant__ Mesh m,
+__global__ void __launch_bounds__(BLOCK) k_resid(const Prm* __restrict__ P, const __grid_constant__ Mesh m,
                                                  const __grid_constant__ State s)
 {
     constexpr int NV = Model<MODEL>::NV, NP = Model<MODEL>::NP;
+    const Prm& p = P[block_solve(s)];
     int c = blockIdx.x * BLOCK + threadIdx.x;
-    bool valid = c < m.nc;
+    bool valid = cell_in(p, c);
     double R[NV];
     if (valid) {
-        double P[NP];
-        loadP<MODEL>(s, m.nc, c, P);
-        gather_residual<MODEL>(p, m, s, c, P, R);
+        double W[NP];
+        loadP<MODEL>(s, m.nc, c, W);
+        gather_residual<MODEL>(p, m, s, c, W, R);
         storeR<MODEL>(s, m.nc, c, R);
     }
     partial_norms<MODEL>(s, valid, R);
@@ -647,13 +676,16 @@ __global__ void __launch_bounds__(BLOCK) k_resid(const __grid_constant__ Prm p, 
 // new, unclamped state) and the residual-norm partial sums of this stage's R (solverCalcRes).
 // ------------------------------------------------------------------------------------------------
 template <int MODEL, bool LAST>
-__global__ void __launch_bounds__(BLOCK) k_rk(const __grid_constant__ Prm p, const __grid_constant__ Mesh m,
+__global__ void __launch_bounds__(BLOCK) k_rk(const Prm* __restrict__ P, const __grid_constant__ Mesh m,
                                               const __grid_constant__ State s, double a)
 {
     constexpr int NV = Model<MODEL>::NV, NP = Model<MODEL>::NP;
-    if (halted(s)) return;
+    const int sid = block_solve(s);
+    const Prm& p = P[sid];
+    Scalars* const sc = s.sc + sid;
+    if (halted(sc)) return;
     int c = blockIdx.x * BLOCK + threadIdx.x;
-    bool valid = c < m.nc;
+    bool valid = cell_in(p, c);
     double R[NV];
     double lmin = bitsd(0x7ff0000000000000ULL);
     if (valid) {
@@ -662,12 +694,12 @@ __global__ void __launch_bounds__(BLOCK) k_rk(const __grid_constant__ Prm p, con
         gather_residual<MODEL>(p, m, s, c, P, R);
         loadU<MODEL>(s, m.nc, c, U);
         double om = m.omega[c];
-        double dt = s.sc->dt_local == 1 ? s.dtl[c] : s.sc->dt;
+        double dt = sc->dt_local == 1 ? s.dtl[c] : sc->dt;
 #pragma unroll
         for (int k = 0; k < NV; k++) U[k] = U[k] - dt * p.sigma * a * R[k] / om;
         if (LAST) {
             double l = local_step<MODEL>(p, U, m.sxh[c], m.syh[c], om);
-            s.dtl[c] = cfl_at(p, s.sc->iter + 1) * l;
+            s.dtl[c] = cfl_at(p, sc->iter + 1) * l;
             lmin = l;
             clamp_prim<MODEL>(p, U, P);
             storeU<MODEL>(s, m.nc, c, U);
@@ -679,7 +711,7 @@ __global__ void __launch_bounds__(BLOCK) k_rk(const __grid_constant__ Prm p, con
     }
     if (LAST) {
         double v = warp_min(lmin);
-        if ((threadIdx.x & 31) == 0 && !(v > bitsd(0x7fefffffffffffffULL))) atomicMin(&s.sc->dtmin_bits, dbits(v));
+        if ((threadIdx.x & 31) == 0 && !(v > bitsd(0x7fefffffffffffffULL))) atomicMin(&sc->dtmin_bits, dbits(v));
         partial_norms<MODEL>(s, valid, R);
     }
 }
@@ -702,13 +734,16 @@ __device__ __forceinline__ void aux_flux(const double* U, double pr, double nx, 
 // off-diagonal blocks of implicitUpdateA (implicit.c:689-813) for each interior face of the cell.
 // ------------------------------------------------------------------------------------------------
 template <int MODEL, bool BLOCKS>
-__global__ void __launch_bounds__(BLOCK) k_impl(const __grid_constant__ Prm p, const __grid_constant__ Mesh m,
+__global__ void __launch_bounds__(BLOCK) k_impl(const Prm* __restrict__ P, const __grid_constant__ Mesh m,
                                                 const __grid_constant__ State s)
 {
     constexpr int NV = Model<MODEL>::NV, NP = Model<MODEL>::NP;
-    if (halted(s)) return;
+    const int sid = block_solve(s);
+    const Prm& p = P[sid];
+    Scalars* const sc = s.sc + sid;
+    if (halted(sc)) return;
     int c = blockIdx.x * BLOCK + threadIdx.x;
-    bool valid = c < m.nc;
+    bool valid = cell_in(p, c);
     double R[NV];
     double lmin = bitsd(0x7ff0000000000000ULL);
     if (valid) {
@@ -834,7 +869,7 @@ __global__ void __launch_bounds__(BLOCK) k_impl(const __grid_constant__ Prm p, c
         }
     }
     double v = warp_min(lmin);
-    if ((threadIdx.x & 31) == 0 && !(v > bitsd(0x7fefffffffffffffULL))) atomicMin(&s.sc->dtmin_bits, dbits(v));
+    if ((threadIdx.x & 31) == 0 && !(v > bitsd(0x7fefffffffffffffULL))) atomicMin(&sc->dtmin_bits, dbits(v));
     partial_norms<MODEL>(s, valid, R);
 }
 
@@ -846,16 +881,19 @@ __global__ void __launch_bounds__(BLOCK) k_impl(const __grid_constant__ Prm p, c
 // (solverUpdateUImplicit, solver.c:1945-1955) and computes the next iteration's primitives.
 // ------------------------------------------------------------------------------------------------
 template <int MODEL, bool LAST>
-__global__ void __launch_bounds__(BLOCK) k_sweep(const __grid_constant__ Prm p, const __grid_constant__ Mesh m,
+__global__ void __launch_bounds__(BLOCK) k_sweep(const Prm* __restrict__ P, const __grid_constant__ Mesh m,
                                                  const __grid_constant__ State s, int sweep, int cur)
 {
     constexpr int NV = Model<MODEL>::NV, NP = Model<MODEL>::NP;
-    if (halted(s)) return;
+    const int sid = block_solve(s);
+    const Prm& p = P[sid];
+    Scalars* const sc = s.sc + sid;
+    if (halted(sc)) return;
     int c = blockIdx.x * BLOCK + threadIdx.x;
     const int nc = m.nc;
-    bool conv = sweep > 0 && bitsd(s.sc->sweep_max[sweep - 1]) < 1e-14;
+    bool conv = sweep > 0 && bitsd(sc->sweep_max[sweep - 1]) < 1e-14;
     double dmax = 0.0;
-    if (c < nc) {
+    if (cell_in(p, c)) {
         const double4* xo4 = s.X4[cur];
         const double* xox = s.Xx[cur];
         double4* xn4 = s.X4[cur ^ 1];
@@ -871,8 +909,8 @@ __global__ void __launch_bounds__(BLOCK) k_sweep(const __grid_constant__ Prm p, 
 #pragma unroll
             for (int k = 0; k < NV; k++) xn[k] = xo[k];
         } else {
-            double cfl = cfl_at(p, s.sc->iter);
-            double dt = p.implicit_local_dt ? s.dtl[c] * cfl : bitsd(s.sc->dtmin_bits) * cfl;
+            double cfl = cfl_at(p, sc->iter);
+            double dt = p.implicit_local_dt ? s.dtl[c] * cfl : bitsd(sc->dtmin_bits) * cfl;
             double D = s.dpart[c] + m.omega[c] / dt;
             double y[NV];
 #pragma unroll
@@ -930,7 +968,7 @@ __global__ void __launch_bounds__(BLOCK) k_sweep(const __grid_constant__ Prm p, 
     }
     if (!conv) {
         double v = warp_max(dmax);
-        if ((threadIdx.x & 31) == 0) atomicMax(&s.sc->sweep_max[sweep], dbits(v));
+        if ((threadIdx.x & 31) == 0) atomicMax(&sc->sweep_max[sweep], dbits(v));
     }
 }
 
@@ -997,20 +1035,23 @@ __device__ __forceinline__ void delta_flux(const Prm& p, const double* P, const 
 //   BWD: x1_i = (D_i x0_i - sum_{higher} 0.5 (dF(x1_j) dS - ra_j x1_j)) / D_i
 // ------------------------------------------------------------------------------------------------
 template <int MODEL, bool FWD>
-__global__ void __launch_bounds__(BLOCK) k_lusgs(const __grid_constant__ Prm p, const __grid_constant__ Mesh m,
+__global__ void __launch_bounds__(BLOCK) k_lusgs(const Prm* __restrict__ P, const __grid_constant__ Mesh m,
                                                  const __grid_constant__ State s, const int* color,
                                                  const int* cells, int mycolor, int start, int count)
 {
     constexpr int NV = Model<MODEL>::NV, NP = Model<MODEL>::NP;
-    if (halted(s)) return;
     int t = blockIdx.x * BLOCK + threadIdx.x;
     if (t >= count) return;
     const int nc = m.nc;
     int c = cells[start + t];
+    const int sid = cell_solve(s, c);
+    const Prm& p = P[sid];
+    Scalars* const sc = s.sc + sid;
+    if (halted(sc)) return;
     const double4* src4 = FWD ? s.X4[0] : s.X4[1];
     const double* srcx = FWD ? s.Xx[0] : s.Xx[1];
-    double cfl = cfl_at(p, s.sc->iter);
-    double dt = p.implicit_local_dt ? s.dtl[c] * cfl : bitsd(s.sc->dtmin_bits) * cfl;
+    double cfl = cfl_at(p, sc->iter);
+    double dt = p.implicit_local_dt ? s.dtl[c] * cfl : bitsd(sc->dtmin_bits) * cfl;
     double D = s.dpart[c] + m.omega[c] / dt;
     double x[NV];
     if (FWD) {
@@ -1070,23 +1111,24 @@ __global__ void __launch_bounds__(BLOCK) k_lusgs(const __grid_constant__ Prm p, 
 
 // U += dW1 (solverUpdateUImplicit), then the next iteration's primitives and clamps
 template <int MODEL>
-__global__ void __launch_bounds__(BLOCK) k_update(const __grid_constant__ Prm p, const __grid_constant__ Mesh m,
+__global__ void __launch_bounds__(BLOCK) k_update(const Prm* __restrict__ P, const __grid_constant__ Mesh m,
                                                   const __grid_constant__ State s)
 {
     constexpr int NV = Model<MODEL>::NV, NP = Model<MODEL>::NP;
-    if (halted(s)) return;
+    const Prm& p = P[block_solve(s)];
+    if (halted(s.sc + block_solve(s))) return;
     int c = blockIdx.x * BLOCK + threadIdx.x;
-    if (c >= m.nc) return;
+    if (!cell_in(p, c)) return;
     const int nc = m.nc;
-    double U[NV], P[NP];
+    double U[NV], W[NP];
     loadU<MODEL>(s, nc, c, U);
     double4 t4 = s.X4[1][c];
     U[0] += t4.x; U[1] += t4.y; U[2] += t4.z; U[3] += t4.w;
 #pragma unroll
     for (int k = 4; k < NV; k++) U[k] += s.Xx[1][(size_t)(k - 4) * nc + c];
-    clamp_prim<MODEL>(p, U, P);
+    clamp_prim<MODEL>(p, U, W);
     storeU<MODEL>(s, nc, c, U);
-    storeP<MODEL>(s, nc, c, P);
+    storeP<MODEL>(s, nc, c, W);
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -1095,14 +1137,18 @@ __global__ void __launch_bounds__(BLOCK) k_update(const __grid_constant__ Prm p,
 // 3 residual only (norms).
 // ------------------------------------------------------------------------------------------------
 template <int MODEL>
-__global__ void __launch_bounds__(BLOCK) k_finalize(const __grid_constant__ Prm p, const __grid_constant__ Mesh m,
-                                                    const __grid_constant__ State s, int npart, int nwall,
-                                                    int mode, int hist_cap)
+__global__ void __launch_bounds__(BLOCK) k_finalize(const Prm* __restrict__ P, const __grid_constant__ Mesh m,
+                                                    const __grid_constant__ State s, int mode)
 {
     constexpr int NV = Model<MODEL>::NV;
     __shared__ double sh[NV + 4][BLOCK / 32];
-    Scalars* sc = s.sc;
-    if (mode != 2 && mode != 3 && halted(s)) return;
+    const int sid = blockIdx.x; // one block per solve
+    const Prm& p = P[sid];
+    Scalars* const sc = s.sc + sid;
+    const int npart = p.nblk, nwall = p.nwall;
+    const double* part = s.part + (size_t)p.blk0 * NV;
+    const double* bcoef = s.bcoef + (size_t)p.wall0 * 4;
+    if (mode != 2 && mode != 3 && halted(sc)) return;
     double v[NV + 4];
 #pragma unroll
     for (int k = 0; k < NV + 4; k++) v[k] = 0.0;
@@ -1111,18 +1157,18 @@ __global__ void __launch_bounds__(BLOCK) k_finalize(const __grid_constant__ Prm 
         int per = (npart + BLOCK - 1) / BLOCK;
         for (int i = threadIdx.x * per; i < min(npart, (int)(threadIdx.x + 1) * per); i++)
 #pragma unroll
-            for (int k = 0; k < NV; k++) v[k] += s.part[(size_t)i * NV + k];
+            for (int k = 0; k < NV; k++) v[k] += part[(size_t)i * NV + k];
         int perw = (nwall + BLOCK - 1) / BLOCK;
         for (int i = threadIdx.x * perw; i < min(nwall, (int)(threadIdx.x + 1) * perw); i++)
 #pragma unroll
-            for (int k = 0; k < 4; k++) v[NV + k] += s.bcoef[(size_t)i * 4 + k];
+            for (int k = 0; k < 4; k++) v[NV + k] += bcoef[(size_t)i * 4 + k];
     }
     block_sum<NV + 4>(v, sh);
     if (threadIdx.x != 0) return;
     if (mode != 2) {
         bool bad = false;
         for (int k = 0; k < NV; k++) {
-            sc->res[k] = sqrt(v[k] / m.nc);
+            sc->res[k] = sqrt(v[k] / p.nc);
             if (!isfinite(sc->res[k])) bad = true;
         }
         // Cx_v -= fx/q per wall face (solver.c:1376-1380): the negated sum
@@ -1134,8 +1180,8 @@ __global__ void __launch_bounds__(BLOCK) k_finalize(const __grid_constant__ Prm 
         }
         sc->coef[0] = cxp; sc->coef[1] = cxv; sc->coef[2] = cyp; sc->coef[3] = cyv;
         if (mode == 3) return;
-        if (s.hist && sc->hist_row < hist_cap) {
-            double* row = s.hist + (size_t)sc->hist_row * (NV + 4);
+        if (sc->hist && sc->hist_row < sc->hist_cap) {
+            double* row = sc->hist + (size_t)sc->hist_row * (NV + 4);
             for (int k = 0; k < NV; k++) row[k] = sc->res[k];
             row[NV] = cxp; row[NV + 1] = cxv; row[NV + 2] = cyp; row[NV + 3] = cyv;
         }
