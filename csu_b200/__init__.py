@@ -95,8 +95,26 @@ def lib():
         L.csu_set_stream.argtypes = [vp, vp]
         L.csu_time_kernels.argtypes = [vp, C.c_int, dp, ip]
         L.csu_residual_norms_noalloc.argtypes = [vp, C.c_int, C.c_int, vp, vp]
+        L.csu_prep_create.argtypes = [C.POINTER(MeshDesc), C.POINTER(Config), C.POINTER(vp)]
+        L.csu_prep_bytes.argtypes = [vp]
+        L.csu_prep_bytes.restype = C.c_longlong
+        L.csu_prep_cells.argtypes = [vp]
+        L.csu_prep_destroy.argtypes = [vp]
+        L.csu_prep_destroy.restype = None
+        L.csu_pack_create.argtypes = [C.POINTER(vp), C.c_int, C.POINTER(vp)]
+        L.csu_pack_size.argtypes = [vp]
+        L.csu_pack_set_state.argtypes = [vp, C.c_int, vp]
+        L.csu_pack_get_state.argtypes = [vp, C.c_int, vp]
+        L.csu_pack_info.argtypes = [vp, C.c_int, C.POINTER(SolveInfo)]
+        L.csu_pack_history.argtypes = [vp, C.c_int, vp, C.c_int, ip]
+        L.csu_pack_transfer.argtypes = [vp, C.c_int, vp, C.c_int]
         _lib = L
     return _lib
+
+
+class SolveInfo(C.Structure):
+    _fields_ = [("iter", C.c_int), ("status", C.c_int), ("done", C.c_int), ("hist_rows", C.c_int),
+                ("have_res0", C.c_int), ("res0", C.c_double * 6), ("res", C.c_double * 6), ("coef", C.c_double * 4)]
 
 
 def _check(st):
@@ -244,6 +262,93 @@ class Engine:
         cnt = (C.c_int * 8)()
         _check(lib().csu_time_kernels(self._h, iters, ms, cnt))
         return {"ms": list(ms), "count": list(cnt)}
+
+    def stats(self):
+        a, b = C.c_longlong(), C.c_longlong()
+        _check(lib().csu_stats(self._h, C.byref(a), C.byref(b)))
+        return {"kernel_launches": a.value, "device_bytes": b.value}
+
+    def close(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.csu_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+class Prep:
+    """A solve prepared on the host for packing (device layout and byte count; no device memory)."""
+
+    def __init__(self, case, config=None, state=None):
+        self.case = case
+        self.config = config if config is not None else case.config
+        self.nvar = self.config.nvar
+        self.n_cells = case.n_cells
+        self.state = np.ascontiguousarray(case.initial_state() if state is None else state, dtype=np.float64)
+        h = C.c_void_p()
+        _check(lib().csu_prep_create(C.byref(case.desc), C.byref(self.config), C.byref(h)))
+        self._h = h
+
+    @property
+    def bytes(self):
+        return lib().csu_prep_bytes(self._h)
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.csu_prep_destroy(self._h)
+            self._h = None
+
+
+class Pack:
+    """Several steady solves advanced together: one launch of each kernel per iteration for all of them."""
+
+    def __init__(self, preps, states=True):
+        self.preps = list(preps)
+        arr = (C.c_void_p * len(self.preps))(*[p._h.value for p in self.preps])
+        h = C.c_void_p()
+        _check(lib().csu_pack_create(arr, len(self.preps), C.byref(h)))
+        self._h = h
+        if states:
+            for k, p in enumerate(self.preps):
+                self.set_state(k, p.state)
+
+    def __len__(self):
+        return len(self.preps)
+
+    def set_state(self, k, U):
+        p = self.preps[k]
+        U = np.ascontiguousarray(U, dtype=np.float64).reshape(p.nvar, p.n_cells)
+        _check(lib().csu_pack_set_state(self._h, k, _ptr(U)))
+
+    def get_state(self, k):
+        p = self.preps[k]
+        U = np.zeros((p.nvar, p.n_cells))
+        _check(lib().csu_pack_get_state(self._h, k, _ptr(U)))
+        return U
+
+    def iterate(self, n):
+        """n iterations of every solve (converged or failed solves stay frozen)."""
+        _check(lib().csu_iterate(self._h, n, 0, None))
+
+    def info(self, k):
+        i = SolveInfo()
+        _check(lib().csu_pack_info(self._h, k, C.byref(i)))
+        nv = self.preps[k].nvar
+        return {"iter": i.iter, "status": i.status, "done": i.done, "hist_rows": i.hist_rows,
+                "res0": np.array(i.res0[:nv]), "res": np.array(i.res[:nv]), "coef": np.array(i.coef[:]),
+                "have_res0": i.have_res0}
+
+    def history(self, k, max_rows=1 << 20):
+        nv = self.preps[k].nvar
+        rows = self.info(k)["hist_rows"]
+        out = np.zeros((max(min(rows, max_rows), 1), nv + 4))
+        n = C.c_int()
+        _check(lib().csu_pack_history(self._h, k, _ptr(out), min(rows, max_rows), C.byref(n)))
+        return out[:n.value]
+
+    def transfer_from(self, other, k_other, k):
+        _check(lib().csu_pack_transfer(other._h, k_other, self._h, k))
 
     def stats(self):
         a, b = C.c_longlong(), C.c_longlong()

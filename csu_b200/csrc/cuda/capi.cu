@@ -40,6 +40,9 @@ struct csu_ctx {
     std::vector<Prm> prms;   // per solve, mirrored at d_prm
     Prm* d_prm = nullptr;
     double* hist = nullptr;  // nsolve blocks of hist_cap rows
+    // packs: cell / interior-face / boundary-face offsets, cell counts and renumbering of each solve
+    std::vector<int> cell0, face0, bface0, ncs;
+    std::vector<std::vector<int>> n2o;
     Mesh mesh;
     State st;
     Arena arena;
@@ -189,6 +192,8 @@ static void plan(csu_ctx* x, Arena& a)
     s.part = carve<double>(a, (size_t)((nc + BLOCK - 1) / BLOCK) * nv);
     s.bcoef = carve<double>(a, (size_t)4 * (nb > 0 ? nb : 1));
     s.sc = carve<Scalars>(a, x->nsolve);
+    s.bsolve = x->nsolve > 1 ? carve<int>(a, (nc + BLOCK - 1) / BLOCK) : nullptr;
+    s.csolve = x->nsolve > 1 ? carve<int>(a, nc) : nullptr;
     x->d_prm = carve<Prm>(a, x->nsolve);
     s.dbg_ghost = carve<double>(a, (size_t)(nb > 0 ? nb : 1) * (nv + 1));
     s.lsq_x87 = carve<unsigned long long>(a, 1);
@@ -218,17 +223,33 @@ static int upload_mesh(csu_ctx* x)
         bd[b] = make_double2(L.bdx[b], L.bdy[b]);
         bun[b] = make_double2(L.bunx[b], L.buny[b]);
     }
-    // walls in reference order (solverCalcCoeff3 sums over wall markers, marker-major)
+    // walls in reference order (solverCalcCoeff3 sums over wall markers, marker-major), per solve
     std::vector<int> rank(nb > 0 ? nb : 1, -1);
     {
-        std::vector<int> by_old(nb, -1);
-        for (int b = 0; b < nb; b++) by_old[L.bold[b]] = b;
         int r = 0;
-        for (int o = 0; o < nb; o++) {
-            int b = by_old[o];
-            if (L.bflag[b] == CSU_BC_WALL || L.bflag[b] == CSU_BC_WALLT) rank[b] = r++;
+        for (int k = 0; k < x->nsolve; k++) {
+            int b0 = x->bface0[k], nbk = (k + 1 < x->nsolve ? x->bface0[k + 1] : nb) - b0;
+            std::vector<int> by_old(nbk, -1);
+            for (int b = 0; b < nbk; b++) by_old[L.bold[b0 + b]] = b0 + b;
+            x->prms[k].wall0 = r;
+            for (int o = 0; o < nbk; o++) {
+                int b = by_old[o];
+                if (L.bflag[b] == CSU_BC_WALL || L.bflag[b] == CSU_BC_WALLT) rank[b] = r++;
+            }
+            x->prms[k].nwall = r - x->prms[k].wall0;
         }
         x->nwall = r;
+    }
+    if (x->nsolve > 1) {
+        int nblk = (nc + BLOCK - 1) / BLOCK;
+        std::vector<int> bs(nblk, 0), cs(nc, 0);
+        for (int k = 0; k < x->nsolve; k++) {
+            int c1 = k + 1 < x->nsolve ? x->cell0[k + 1] : nc;
+            for (int c = x->cell0[k]; c < c1; c++) cs[c] = k;
+            for (int b = x->cell0[k] / BLOCK; b < (c1 + BLOCK - 1) / BLOCK; b++) bs[b] = k;
+        }
+        CK(up(x->st.bsolve, bs.data(), sizeof(int) * nblk));
+        CK(up(x->st.csolve, cs.data(), sizeof(int) * nc));
     }
     CK(up(m.npts, L.npts, sizeof(int) * nc));
     CK(up(m.nint, L.nint, sizeof(int) * nc));
@@ -272,19 +293,17 @@ static int upload_mesh(csu_ctx* x)
     return CSU_OK;
 }
 
-static void fill_params(csu_ctx* x)
+static void fill_params_from(const csu_config& c, const csu_layout& L, Prm& p)
 {
-    const csu_config& c = x->cfg;
-    Prm& p = x->prm;
     memset(&p, 0, sizeof(p));
     p.gas.gamma = c.gamma;
     p.gas.R = c.gas_r;
     p.gas.Cp = c.gamma * c.gas_r / (c.gamma - 1); // gaspropInit (gasprop.c:14-37)
     p.gas.Cv = p.gas.Cp - c.gas_r;
     p.gas.tp = c.tp;
-    p.nc = x->L.nc;
-    p.nf = x->L.nf;
-    p.nb = x->L.nb;
+    p.nc = L.nc;
+    p.nf = L.nf;
+    p.nb = L.nb;
     p.order = c.order;
     p.scheme = c.flux;
     p.laminar = c.laminar;
@@ -298,7 +317,7 @@ static void fill_params(csu_ctx* x)
     p.tube = c.tube;
     p.n_linear = c.n_linear;
     p.lim_k = c.limiter_k;
-    p.vol_max = x->L.vol_max;
+    p.vol_max = L.vol_max;
     p.e_fix = c.e_fix;
     p.r_lim = c.r_lim;
     p.p_out = c.p_out;
@@ -316,7 +335,7 @@ static void fill_params(csu_ctx* x)
     p.pref20[1] = c.pin[1] * c.pin[1] + c.pin[2] * c.pin[2];
     p.pref20[2] = p.pref20[1];
     p.pref20[3] = c.pin[3] * c.pin[3];
-    for (int k = 4; k < x->nv; k++) p.pref20[k] = c.pin[k + 1] * c.pin[k + 1];
+    for (int k = 4; k < c.nvar; k++) p.pref20[k] = c.pin[k + 1] * c.pin[k + 1];
     // solverCalcCoeff3 (solver.c:1348-1352)
     p.p_inf = c.pin[3];
     p.q_inf = 0.5 * c.pin[0] * (c.pin[1] * c.pin[1] + c.pin[2] * c.pin[2]);
@@ -363,6 +382,7 @@ static int reset_scalars(csu_ctx* x, int it0)
         h.dtmin_bits = 0x7ff0000000000000ULL;
         h.dt_local = x->cfg.dt_local;
         h.iter = it0;
+        h.fresh = 1;
         h.hist = hist_of(x, k);
         h.hist_cap = x->hist_cap;
     }
@@ -399,6 +419,86 @@ static int upload_prm(csu_ctx* x)
     return CSU_OK;
 }
 
+// The settings this engine runs (csu_create's checks); sets the model (0 Euler/laminar, 1 SA, 2 SST).
+static int validate_config(const char* who, const csu_config* cfg, int* model_out, int* nv_out)
+{
+    int model = cfg->sst ? 2 : (cfg->sa ? 1 : 0);
+    int nv = model == 0 ? 4 : (model == 1 ? 5 : 6);
+    if (cfg->nvar != nv) {
+        csu_set_error("%s: nvar %d does not match the turbulence model", who, cfg->nvar);
+        return CSU_ERR_INPUT;
+    }
+    if (model == 2 && (cfg->flux == CSU_FLUX_ROE || cfg->sst_trans || cfg->time_scheme != CSU_TS_RK)) {
+        csu_set_error("%s: SST supports RK time stepping with the AUSM family (the reference has no Roe "
+                      "branch for SST and calls 4x4 DPLUR blocks with 6 variables); sstTrans not yet available", who);
+        return CSU_ERR_UNSUPPORTED;
+    }
+    if (model == 1 && (cfg->flux == CSU_FLUX_ROE || cfg->sa_cc)) {
+        csu_set_error("%s: SA with %s is not available (the reference has no Roe branch for SA)", who,
+                      cfg->sa_cc ? "saCC" : "Roe");
+        return CSU_ERR_UNSUPPORTED;
+    }
+    if (cfg->time_scheme == CSU_TS_LUSGS && model == 2) {
+        csu_set_error("%s: LU-SGS with SST is not available in this engine build", who);
+        return CSU_ERR_UNSUPPORTED;
+    }
+    if (cfg->time_scheme == CSU_TS_RK && !(cfg->stages == 1 || cfg->stages == 3 || cfg->stages == 4 ||
+                                            cfg->stages == 5)) {
+        csu_set_error("%s: RK with %d stages (the reference implements 1, 3, 4, 5)", who, cfg->stages);
+        return CSU_ERR_UNSUPPORTED;
+    }
+    if (cfg->time_scheme == CSU_TS_DPLUR && (cfg->n_linear < 1 || cfg->n_linear > MAX_SWEEPS)) {
+        csu_set_error("%s: Nlinear must be in [1, %d]", who, MAX_SWEEPS);
+        return CSU_ERR_UNSUPPORTED;
+    }
+    if (cfg->order != 1 && cfg->order != 2) {
+        csu_set_error("%s: order must be 1 or 2", who);
+        return CSU_ERR_INPUT;
+    }
+    if (cfg->limiter_type != 0) {
+        csu_set_error("%s: limiter type %d not available in this engine build", who, cfg->limiter_type);
+        return CSU_ERR_UNSUPPORTED;
+    }
+    *model_out = model;
+    *nv_out = nv;
+    return CSU_OK;
+}
+
+// Allocates and fills the device side of x (x->L, x->prms and the pack offsets set by the caller).
+static int ctx_setup(csu_ctx* x)
+{
+    int st;
+    x->mesh.nc = x->L.nc;
+    x->mesh.nf = x->L.nf;
+    x->mesh.nb = x->L.nb;
+    // size, allocate once, carve
+    Arena a;
+    plan(x, a);
+    size_t bytes = a.size;
+    cudaError_t e = cudaMalloc((void**)&x->arena.base, bytes);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(context arena)");
+    x->arena.size = bytes;
+    x->arena.used = 0;
+    plan(x, x->arena);
+    e = cudaMemset(x->arena.base, 0, bytes);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&x->own_stream, cudaStreamNonBlocking);
+    x->stream = x->own_stream;
+    if (e != cudaSuccess) return cuda_fail(e, "context setup");
+    x->gb_c = (x->L.nc + BLOCK - 1) / BLOCK;
+    x->gb_fi = (x->L.nf + BLOCK - 1) / BLOCK;
+    x->gb_fb = (x->L.nb + BLOCK - 1) / BLOCK;
+    if ((st = upload_mesh(x))) return st;
+    x->prm = x->prms[0];
+    if ((st = upload_prm(x)) || (st = reset_scalars(x, 0))) return st;
+    switch (x->cfg.stages) {
+    case 1: x->rk = RK1; break;
+    case 3: x->rk = RK3; break;
+    case 4: x->rk = RK4; break;
+    default: x->rk = RK5; break;
+    }
+    return CSU_OK;
+}
+
 extern "C" int csu_create(const csu_mesh_desc* md, const csu_config* cfg, csu_ctx** out)
 {
     *out = nullptr;
@@ -406,43 +506,9 @@ extern "C" int csu_create(const csu_mesh_desc* md, const csu_config* cfg, csu_ct
         csu_set_error("csu_create: empty mesh or missing config");
         return CSU_ERR_INPUT;
     }
-    int model = cfg->sst ? 2 : (cfg->sa ? 1 : 0);
-    int nv = model == 0 ? 4 : (model == 1 ? 5 : 6);
-    if (cfg->nvar != nv) {
-        csu_set_error("csu_create: nvar %d does not match the turbulence model", cfg->nvar);
-        return CSU_ERR_INPUT;
-    }
-    if (model == 2 && (cfg->flux == CSU_FLUX_ROE || cfg->sst_trans || cfg->time_scheme != CSU_TS_RK)) {
-        csu_set_error("csu_create: SST supports RK time stepping with the AUSM family (the reference has no Roe "
-                      "branch for SST and calls 4x4 DPLUR blocks with 6 variables); sstTrans not yet available");
-        return CSU_ERR_UNSUPPORTED;
-    }
-    if (model == 1 && (cfg->flux == CSU_FLUX_ROE || cfg->sa_cc)) {
-        csu_set_error("csu_create: SA with %s is not available (the reference has no Roe branch for SA)",
-                      cfg->sa_cc ? "saCC" : "Roe");
-        return CSU_ERR_UNSUPPORTED;
-    }
-    if (cfg->time_scheme == CSU_TS_LUSGS && model == 2) {
-        csu_set_error("csu_create: LU-SGS with SST is not available in this engine build");
-        return CSU_ERR_UNSUPPORTED;
-    }
-    if (cfg->time_scheme == CSU_TS_RK && !(cfg->stages == 1 || cfg->stages == 3 || cfg->stages == 4 ||
-                                            cfg->stages == 5)) {
-        csu_set_error("csu_create: RK with %d stages (the reference implements 1, 3, 4, 5)", cfg->stages);
-        return CSU_ERR_UNSUPPORTED;
-    }
-    if (cfg->time_scheme == CSU_TS_DPLUR && (cfg->n_linear < 1 || cfg->n_linear > MAX_SWEEPS)) {
-        csu_set_error("csu_create: Nlinear must be in [1, %d]", MAX_SWEEPS);
-        return CSU_ERR_UNSUPPORTED;
-    }
-    if (cfg->order != 1 && cfg->order != 2) {
-        csu_set_error("csu_create: order must be 1 or 2");
-        return CSU_ERR_INPUT;
-    }
-    if (cfg->limiter_type != 0) {
-        csu_set_error("csu_create: limiter type %d not available in this engine build", cfg->limiter_type);
-        return CSU_ERR_UNSUPPORTED;
-    }
+    int model, nv;
+    int st = validate_config("csu_create", cfg, &model, &nv);
+    if (st) return st;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         csu_set_error("csu_create: no CUDA device");
@@ -452,61 +518,24 @@ extern "C" int csu_create(const csu_mesh_desc* md, const csu_config* cfg, csu_ct
     x->model = model;
     x->nv = nv;
     x->cfg = *cfg;
-    int st = csu_layout_build(md, cfg->axisymmetric, &x->L);
+    st = csu_layout_build(md, cfg->axisymmetric, &x->L);
     if (st) {
         delete x;
         csu_set_error("csu_create: mesh layout failed (a cell with more than four faces?)");
         return st;
     }
-    fill_params(x);
-    x->mesh.nc = x->L.nc;
-    x->mesh.nf = x->L.nf;
-    x->mesh.nb = x->L.nb;
-    // size, allocate once, carve
-    Arena a;
-    plan(x, a);
-    size_t bytes = a.size;
-    cudaError_t e = cudaMalloc((void**)&x->arena.base, bytes);
-    if (e != cudaSuccess) {
-        csu_layout_free(&x->L);
-        delete x;
-        return cuda_fail(e, "cudaMalloc(context arena)");
-    }
-    x->arena.size = bytes;
-    x->arena.used = 0;
-    plan(x, x->arena);
-    e = cudaMemset(x->arena.base, 0, bytes);
-    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&x->own_stream, cudaStreamNonBlocking);
-    x->stream = x->own_stream;
-    if (e != cudaSuccess) {
-        cudaFree(x->arena.base);
-        csu_layout_free(&x->L);
-        delete x;
-        return cuda_fail(e, "context setup");
-    }
-    x->gb_c = (x->L.nc + BLOCK - 1) / BLOCK;
-    if ((st = upload_mesh(x))) {
+    x->cell0 = {0};
+    x->face0 = {0};
+    x->bface0 = {0};
+    x->ncs = {x->L.nc};
+    x->prms.resize(1);
+    fill_params_from(x->cfg, x->L, x->prms[0]);
+    x->prms[0].cell0 = 0;
+    x->prms[0].blk0 = 0;
+    x->prms[0].nblk = (x->L.nc + BLOCK - 1) / BLOCK;
+    if ((st = ctx_setup(x))) {
         csu_destroy(x);
         return st;
-    }
-    x->prm.cell0 = 0;
-    x->prm.blk0 = 0;
-    x->prm.nblk = x->gb_c;
-    x->prm.wall0 = 0;
-    x->prm.nwall = x->nwall;
-    x->prms.assign(1, x->prm);
-    if ((st = upload_prm(x)) || (st = reset_scalars(x, 0))) {
-        csu_destroy(x);
-        return st;
-    }
-
-    x->gb_fi = (x->L.nf + BLOCK - 1) / BLOCK;
-    x->gb_fb = (x->L.nb + BLOCK - 1) / BLOCK;
-    switch (cfg->stages) {
-    case 1: x->rk = RK1; break;
-    case 3: x->rk = RK3; break;
-    case 4: x->rk = RK4; break;
-    default: x->rk = RK5; break;
     }
     *out = x;
     return CSU_OK;
@@ -524,39 +553,68 @@ extern "C" void csu_destroy(csu_ctx* x)
     delete x;
 }
 
+// State of solve k in its reference order ([var][cell], nvar x its cell count), to or from the device.
+static int solve_state_io(csu_ctx* x, int k, double* U, bool put)
+{
+    const int nck = x->ncs[k], o = x->cell0[k], NC = x->L.nc, nv = x->nv;
+    // a pack keeps each solve's renumbering (its concatenated layout has none); a one-solve context its own
+    const int* n2o = x->n2o.empty() ? x->L.cell_new2old : x->n2o[k].data();
+    std::vector<double4> u4(nck);
+    std::vector<double> ux((size_t)(nv - 4) * nck + 1);
+    if (put) {
+        for (int c = 0; c < nck; c++) {
+            int q = n2o[c];
+            u4[c] = make_double4(U[q], U[(size_t)nck + q], U[(size_t)2 * nck + q], U[(size_t)3 * nck + q]);
+            for (int r = 4; r < nv; r++) ux[(size_t)(r - 4) * nck + c] = U[(size_t)r * nck + q];
+        }
+        CK(cudaStreamSynchronize(x->stream));
+        CK(cudaMemcpy(x->st.U4 + o, u4.data(), sizeof(double4) * nck, cudaMemcpyHostToDevice));
+        {
+            Scalars h;
+            CK(cudaMemcpy(&h, x->st.sc + k, sizeof(Scalars), cudaMemcpyDeviceToHost));
+            h.fresh = 1;
+            CK(cudaMemcpy(x->st.sc + k, &h, sizeof(Scalars), cudaMemcpyHostToDevice));
+        }
+        for (int r = 4; r < nv; r++)
+            CK(cudaMemcpy(x->st.Ux + (size_t)(r - 4) * NC + o, ux.data() + (size_t)(r - 4) * nck,
+                          sizeof(double) * nck, cudaMemcpyHostToDevice));
+        x->prepared = 0;
+        return CSU_OK;
+    }
+    CK(cudaStreamSynchronize(x->stream));
+    CK(cudaMemcpy(u4.data(), x->st.U4 + o, sizeof(double4) * nck, cudaMemcpyDeviceToHost));
+    for (int r = 4; r < nv; r++)
+        CK(cudaMemcpy(ux.data() + (size_t)(r - 4) * nck, x->st.Ux + (size_t)(r - 4) * NC + o, sizeof(double) * nck,
+                      cudaMemcpyDeviceToHost));
+    for (int c = 0; c < nck; c++) {
+        int q = n2o[c];
+        U[q] = u4[c].x;
+        U[(size_t)nck + q] = u4[c].y;
+        U[(size_t)2 * nck + q] = u4[c].z;
+        U[(size_t)3 * nck + q] = u4[c].w;
+        for (int r = 4; r < nv; r++) U[(size_t)r * nck + q] = ux[(size_t)(r - 4) * nck + c];
+    }
+    return CSU_OK;
+}
+
 extern "C" int csu_set_state(csu_ctx* x, const double* U)
 {
-    const int nc = x->L.nc, nv = x->nv;
-    std::vector<double4> u4(nc);
-    std::vector<double> ux((size_t)(nv - 4) * nc + 1);
-    for (int c = 0; c < nc; c++) {
-        int o = x->L.cell_new2old[c];
-        u4[c] = make_double4(U[o], U[(size_t)nc + o], U[(size_t)2 * nc + o], U[(size_t)3 * nc + o]);
-        for (int k = 4; k < nv; k++) ux[(size_t)(k - 4) * nc + c] = U[(size_t)k * nc + o];
+    if (!x || !U) return CSU_ERR_INPUT;
+    if (!x->n2o.empty()) {
+        csu_set_error("csu_set_state: a pack holds its solves separately (use csu_pack_set_state)");
+        return CSU_ERR_STATE;
     }
-    CK(cudaMemcpy(x->st.U4, u4.data(), sizeof(double4) * nc, cudaMemcpyHostToDevice));
-    if (nv > 4) CK(cudaMemcpy(x->st.Ux, ux.data(), sizeof(double) * (nv - 4) * nc, cudaMemcpyHostToDevice));
-    x->prepared = 0;
-    return CSU_OK;
+    return solve_state_io(x, 0, const_cast<double*>(U), true);
 }
 
 extern "C" int csu_get_state(csu_ctx* x, double* U)
 {
-    const int nc = x->L.nc, nv = x->nv;
-    std::vector<double4> u4(nc);
-    std::vector<double> ux((size_t)(nv - 4) * nc + 1);
-    CK(cudaStreamSynchronize(x->stream));
-    CK(cudaMemcpy(u4.data(), x->st.U4, sizeof(double4) * nc, cudaMemcpyDeviceToHost));
-    if (nv > 4) CK(cudaMemcpy(ux.data(), x->st.Ux, sizeof(double) * (nv - 4) * nc, cudaMemcpyDeviceToHost));
-    for (int c = 0; c < nc; c++) {
-        int o = x->L.cell_new2old[c];
-        U[o] = u4[c].x;
-        U[(size_t)nc + o] = u4[c].y;
-        U[(size_t)2 * nc + o] = u4[c].z;
-        U[(size_t)3 * nc + o] = u4[c].w;
-        for (int k = 4; k < nv; k++) U[(size_t)k * nc + o] = ux[(size_t)(k - 4) * nc + c];
+    if (!x || !U) return CSU_ERR_INPUT;
+    if (!x->n2o.empty()) {
+        csu_set_error("csu_get_state: a pack holds its solves separately (use csu_pack_get_state)");
+        return CSU_ERR_STATE;
     }
-    return CSU_OK;
+    return solve_state_io(x, 0, U, false);
 }
 
 extern "C" int csu_set_state_rows(csu_ctx* x, const double* const* U)
@@ -619,7 +677,7 @@ template <int MODEL>
 static void launch_prologue(csu_ctx* x)
 {
     int rk = x->cfg.time_scheme == CSU_TS_RK;
-    k_prim<MODEL><<<x->gb_c, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st, rk);
+    k_prim<MODEL><<<x->gb_c, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st, rk, 1);
     x->launches++;
     tmark(x, KPRIM);
     launch_finalize<MODEL>(x, 2);
@@ -688,7 +746,7 @@ static void launch_iteration(csu_ctx* x)
 template <int MODEL>
 static void launch_residual(csu_ctx* x, bool dbg)
 {
-    k_prim<MODEL><<<x->gb_c, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st, 0);
+    k_prim<MODEL><<<x->gb_c, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st, 0, 0);
     x->launches++;
     if (x->cfg.order == 2 || dbg) launch_grad<MODEL>(x, dbg);
     launch_flux<MODEL>(x, 1);
@@ -766,21 +824,24 @@ static int run_iterations(csu_ctx* x, int n, int it0, Scalars* out)
 {
     int st;
     if ((st = ensure_hist(x, n))) return st;
-    if (!x->prepared) {
+    if (!x->prepared && x->nsolve == 1) {
         if ((st = reset_scalars(x, it0))) return st;
-        DISPATCH(launch_prologue, x);
-        if ((st = check_launch("prologue"))) return st;
-        x->prepared = 1;
     } else {
-        // keep the device step state, restart the history rows and the loop counter
+        // keep the device step state, restart the history rows (and, for one solve, the loop counter;
+        // the solves of a pack keep their own)
         std::vector<Scalars> hs(x->nsolve);
         if ((st = read_scalars_n(x, hs.data(), x->nsolve))) return st;
         for (Scalars& h : hs) {
             h.hist_row = 0;
-            h.iter = it0;
+            if (x->nsolve == 1) h.iter = it0;
             h.steps = 0;
         }
         if ((st = write_scalars_n(x, hs.data(), x->nsolve))) return st;
+    }
+    if (!x->prepared) {
+        DISPATCH(launch_prologue, x);
+        if ((st = check_launch("prologue"))) return st;
+        x->prepared = 1;
     }
     // graphs of G iterations; G even so the DPLUR increment buffers come back to the same parity
     const int G = 8;
@@ -809,6 +870,7 @@ extern "C" int csu_iterate_ex(csu_ctx* x, int n, int it0, double* hist, int* n_d
     int st = run_iterations(x, n, it0, &h);
     if (!st && n_done) *n_done = h.steps;
     if (st) return st;
+    if (x->nsolve > 1) return CSU_OK; // per-solve results: csu_pack_info, csu_pack_history
     if (hist) {
         int rows = h.hist_row < n ? h.hist_row : n;
         CK(cudaMemcpy(hist, x->hist, sizeof(double) * (size_t)rows * (x->nv + 4), cudaMemcpyDeviceToHost));
@@ -884,6 +946,11 @@ extern "C" int csu_residual(csu_ctx* x, double* R)
 
 extern "C" int csu_dump(csu_ctx* x, int what, double* out)
 {
+    if (!x || !out) return CSU_ERR_INPUT;
+    if (!x->n2o.empty() && what != CSU_DUMP_LSQ_X87) {
+        csu_set_error("csu_dump: views in reference order are per solve and not available for packs");
+        return CSU_ERR_STATE;
+    }
     const int nc = x->L.nc, nf = x->L.nf, nb = x->L.nb, nv = x->nv, nx = nv - 4;
     CK(cudaStreamSynchronize(x->stream));
     auto d2h = [&](std::vector<double>& v, const void* src, size_t n) -> cudaError_t {
@@ -1052,5 +1119,234 @@ extern "C" int csu_time_kernels(csu_ctx* x, int iters, double* ms, int* count)
             count[k]++;
         }
     }
+    return CSU_OK;
+}
+
+// ------------------------------------------------------------------------------------------------ packs
+
+struct csu_prep {
+    csu_config cfg;
+    csu_layout L;
+    int model = 0, nv = 4;
+    long long bytes = 0;
+};
+
+// Settings every solve of a pack shares (the launch sequence and the kernels' specialisation depend on
+// them); flow conditions, walls' temperature, outlet pressure, CFL schedule, stopping drop and reference
+// length may differ per solve.
+static bool same_structure(const csu_config& a, const csu_config& b)
+{
+    return a.nvar == b.nvar && a.order == b.order && a.flux == b.flux && a.stages == b.stages &&
+           a.time_scheme == b.time_scheme && a.n_linear == b.n_linear && a.dt_local == b.dt_local &&
+           a.dt_local_n == b.dt_local_n && a.laminar == b.laminar && a.sa == b.sa && a.sa_cc == b.sa_cc &&
+           a.sst == b.sst && a.sst_trans == b.sst_trans && a.axisymmetric == b.axisymmetric &&
+           a.turb1order == b.turb1order && a.visc_blazek == b.visc_blazek && a.tp == b.tp &&
+           a.limiter_type == b.limiter_type && a.tube == b.tube && a.implicit_fp32 == b.implicit_fp32 &&
+           a.implicit_local_dt == b.implicit_local_dt;
+}
+
+extern "C" int csu_prep_create(const csu_mesh_desc* md, const csu_config* cfg, csu_prep** out)
+{
+    if (!out) return CSU_ERR_INPUT;
+    *out = nullptr;
+    if (!md || !cfg || md->n_cells <= 0) {
+        csu_set_error("csu_prep_create: empty mesh or missing config");
+        return CSU_ERR_INPUT;
+    }
+    int model, nv;
+    int st = validate_config("csu_prep_create", cfg, &model, &nv);
+    if (st) return st;
+    csu_prep* p = new csu_prep();
+    p->cfg = *cfg;
+    p->model = model;
+    p->nv = nv;
+    st = csu_layout_build(md, cfg->axisymmetric, &p->L);
+    if (st) {
+        delete p;
+        csu_set_error("csu_prep_create: mesh layout failed (a cell with more than four faces?)");
+        return st;
+    }
+    // device bytes of the solve: the arena a one-solve context would carve, plus 1024 history rows
+    csu_ctx t;
+    t.model = model;
+    t.nv = nv;
+    t.cfg = *cfg;
+    t.L = p->L;
+    Arena a;
+    plan(&t, a);
+    memset(&t.L, 0, sizeof(t.L)); // owned by p
+    p->bytes = (long long)a.size + 1024LL * (nv + 4) * 8;
+    *out = p;
+    return CSU_OK;
+}
+
+extern "C" long long csu_prep_bytes(const csu_prep* p)
+{
+    return p ? p->bytes : 0;
+}
+
+extern "C" int csu_prep_cells(const csu_prep* p)
+{
+    return p ? p->L.nc : 0;
+}
+
+extern "C" void csu_prep_destroy(csu_prep* p)
+{
+    if (!p) return;
+    csu_layout_free(&p->L);
+    delete p;
+}
+
+extern "C" int csu_pack_create(const csu_prep* const* solves, int n, csu_ctx** out)
+{
+    if (!out) return CSU_ERR_INPUT;
+    *out = nullptr;
+    if (!solves || n < 1) {
+        csu_set_error("csu_pack_create: no solves");
+        return CSU_ERR_INPUT;
+    }
+    for (int k = 0; k < n; k++) {
+        if (!solves[k]) return CSU_ERR_INPUT;
+        if (!same_structure(solves[0]->cfg, solves[k]->cfg)) {
+            csu_set_error("csu_pack_create: solve %d differs from solve 0 in a setting a pack shares (model, "
+                          "scheme, order, time stepping, ...)", k);
+            return CSU_ERR_INPUT;
+        }
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        csu_set_error("csu_pack_create: no CUDA device");
+        return CSU_ERR_NO_DEVICE;
+    }
+    csu_ctx* x = new csu_ctx();
+    x->model = solves[0]->model;
+    x->nv = solves[0]->nv;
+    x->cfg = solves[0]->cfg;
+    x->nsolve = n;
+    std::vector<const csu_layout*> parts(n);
+    for (int k = 0; k < n; k++) parts[k] = &solves[k]->L;
+    x->cell0.resize(n);
+    x->face0.resize(n);
+    x->bface0.resize(n);
+    int st = csu_layout_concat(parts.data(), n, BLOCK, &x->L, x->cell0.data(), x->face0.data(), x->bface0.data());
+    if (st) {
+        delete x;
+        csu_set_error("csu_pack_create: layouts could not be packed");
+        return st;
+    }
+    x->prms.resize(n);
+    x->ncs.resize(n);
+    x->n2o.resize(n);
+    for (int k = 0; k < n; k++) {
+        const csu_layout& L = solves[k]->L;
+        fill_params_from(solves[k]->cfg, L, x->prms[k]);
+        x->prms[k].cell0 = x->cell0[k];
+        x->prms[k].blk0 = x->cell0[k] / BLOCK;
+        x->prms[k].nblk = (L.nc + BLOCK - 1) / BLOCK;
+        x->ncs[k] = L.nc;
+        x->n2o[k].assign(L.cell_new2old, L.cell_new2old + L.nc);
+    }
+    if ((st = ctx_setup(x))) {
+        csu_destroy(x);
+        return st;
+    }
+    *out = x;
+    return CSU_OK;
+}
+
+extern "C" int csu_pack_size(csu_ctx* x)
+{
+    return x ? x->nsolve : 0;
+}
+
+extern "C" int csu_pack_set_state(csu_ctx* x, int k, const double* U)
+{
+    if (!x || !U || k < 0 || k >= x->nsolve) return CSU_ERR_INPUT;
+    return solve_state_io(x, k, const_cast<double*>(U), true);
+}
+
+extern "C" int csu_pack_get_state(csu_ctx* x, int k, double* U)
+{
+    if (!x || !U || k < 0 || k >= x->nsolve) return CSU_ERR_INPUT;
+    return solve_state_io(x, k, U, false);
+}
+
+extern "C" int csu_pack_info(csu_ctx* x, int k, csu_solve_info* info)
+{
+    if (!x || !info || k < 0 || k >= x->nsolve) return CSU_ERR_INPUT;
+    std::vector<Scalars> hs(x->nsolve);
+    int st = read_scalars_n(x, hs.data(), x->nsolve);
+    if (st) return st;
+    const Scalars& h = hs[k];
+    memset(info, 0, sizeof(*info));
+    info->iter = h.iter;
+    info->status = h.status;
+    info->done = h.done;
+    info->hist_rows = h.hist_row < h.hist_cap ? h.hist_row : h.hist_cap;
+    info->have_res0 = h.have_res0;
+    for (int v = 0; v < x->nv; v++) {
+        info->res0[v] = h.res0[v];
+        info->res[v] = h.res[v];
+    }
+    for (int v = 0; v < 4; v++) info->coef[v] = h.coef[v];
+    return CSU_OK;
+}
+
+extern "C" int csu_pack_history(csu_ctx* x, int k, double* hist, int max_rows, int* rows)
+{
+    if (!x || !hist || k < 0 || k >= x->nsolve) return CSU_ERR_INPUT;
+    csu_solve_info info;
+    int st = csu_pack_info(x, k, &info);
+    if (st) return st;
+    int n = info.hist_rows < max_rows ? info.hist_rows : max_rows;
+    if (n > 0) CK(cudaMemcpy(hist, hist_of(x, k), sizeof(double) * (size_t)n * (x->nv + 4), cudaMemcpyDeviceToHost));
+    if (rows) *rows = n;
+    return CSU_OK;
+}
+
+// Device copy of solve kf of `from` into solve kt of `to` (same mesh and settings): conserved state,
+// primitives, the implicit increments (DPLUR warm start) and the solve's counters, first residual and
+// flags, so that `to` continues the solve where `from` left it.
+extern "C" int csu_pack_transfer(csu_ctx* from, int kf, csu_ctx* to, int kt)
+{
+    if (!from || !to || kf < 0 || kf >= from->nsolve || kt < 0 || kt >= to->nsolve) return CSU_ERR_INPUT;
+    if (from->model != to->model || from->ncs[kf] != to->ncs[kt] || !same_structure(from->cfg, to->cfg)) {
+        csu_set_error("csu_pack_transfer: the two solves differ in size or settings");
+        return CSU_ERR_INPUT;
+    }
+    const int n = from->ncs[kf], of = from->cell0[kf], ot = to->cell0[kt], NF = from->L.nc, NT = to->L.nc;
+    const int nx = from->nv - 4;
+    CK(cudaStreamSynchronize(from->stream));
+    CK(cudaStreamSynchronize(to->stream));
+    auto cp = [&](void* dst, const void* src, size_t bytes) { return cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToDevice); };
+    CK(cp(to->st.U4 + ot, from->st.U4 + of, sizeof(double4) * n));
+    CK(cp(to->st.W4 + ot, from->st.W4 + of, sizeof(double4) * n));
+    CK(cp(to->st.WT + ot, from->st.WT + of, sizeof(double) * n));
+    CK(cp(to->st.dtl + ot, from->st.dtl + of, sizeof(double) * n));
+    for (int r = 0; r < nx; r++) {
+        CK(cp(to->st.Ux + (size_t)r * NT + ot, from->st.Ux + (size_t)r * NF + of, sizeof(double) * n));
+        CK(cp(to->st.Wx + (size_t)r * NT + ot, from->st.Wx + (size_t)r * NF + of, sizeof(double) * n));
+    }
+    if (from->st.X4[0] && to->st.X4[0]) {
+        for (int q = 0; q < 2; q++) {
+            int qf = from->xcur ^ q, qt = to->xcur ^ q;
+            CK(cp(to->st.X4[qt] + ot, from->st.X4[qf] + of, sizeof(double4) * n));
+            for (int r = 0; r < nx; r++)
+                CK(cp(to->st.Xx[qt] + (size_t)r * NT + ot, from->st.Xx[qf] + (size_t)r * NF + of, sizeof(double) * n));
+        }
+    }
+    Scalars hf, ht;
+    CK(cudaMemcpy(&hf, from->st.sc + kf, sizeof(Scalars), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&ht, to->st.sc + kt, sizeof(Scalars), cudaMemcpyDeviceToHost));
+    double* hist = ht.hist;
+    int cap = ht.hist_cap;
+    ht = hf;
+    ht.hist = hist;
+    ht.hist_cap = cap;
+    ht.hist_row = 0;
+    ht.steps = 0;
+    ht.fresh = 0;
+    CK(cudaMemcpy(to->st.sc + kt, &ht, sizeof(Scalars), cudaMemcpyHostToDevice));
+    to->prepared = 0;
     return CSU_OK;
 }

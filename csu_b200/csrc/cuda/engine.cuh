@@ -65,6 +65,7 @@ struct Scalars {
     int hist_row;                         // next history row
     int steps;                            // iterations completed in this call
     int have_res0;                        // res0 recorded
+    int fresh;                            // state set from outside: the prologue derives W and the step
     int hist_cap;                         // rows available at hist
     double* hist;                         // history rows of this solve (or null)
 };

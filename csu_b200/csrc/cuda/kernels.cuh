@@ -47,12 +47,14 @@ __device__ __forceinline__ bool cell_in(const Prm& p, int c)
 // ------------------------------------------------------------------------------------------------
 template <int MODEL>
 __global__ void __launch_bounds__(BLOCK) k_prim(const Prm* __restrict__ P, const __grid_constant__ Mesh m,
-                                                const __grid_constant__ State s, int with_dt)
+                                                const __grid_constant__ State s, int with_dt, int only_fresh)
 {
     constexpr int NV = Model<MODEL>::NV, NP = Model<MODEL>::NP;
     const int sid = block_solve(s);
     const Prm& p = P[sid];
     Scalars* const sc = s.sc + sid;
+    // prologue of a pack: solves carried over from another pack keep their primitives and step
+    if (only_fresh && !sc->fresh) return;
     int c = blockIdx.x * BLOCK + threadIdx.x;
     double lmin = __longlong_as_double(0x7ff0000000000000LL);
     if (cell_in(p, c)) {
@@ -1201,6 +1203,11 @@ __global__ void __launch_bounds__(BLOCK) k_finalize(const Prm* __restrict__ P, c
         if (p.conv_tol > 0 && sc->res[0] <= p.conv_tol * sc->res0[0]) sc->done = 1;
         for (int k = 0; k < MAX_SWEEPS; k++) sc->sweep_max[k] = 0ULL;
     }
+    if (mode == 2 && !sc->fresh) {
+        sc->dtmin_bits = 0x7ff0000000000000ULL;
+        return;
+    }
+    if (mode == 2) sc->fresh = 0;
     if (mode == 0 || mode == 2) {
         // solverCalcDt (solver.c:925-950) for the next iteration, from the minimum gathered above
         double dt = bitsd(sc->dtmin_bits);

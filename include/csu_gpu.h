@@ -230,6 +230,39 @@ int csu_residual_norms_noalloc(const double* R, int nvar, int ncells, double* re
 /* Counters of the engine: kernels launched since creation, device bytes held. */
 int csu_stats(csu_ctx* ctx, long long* kernel_launches, long long* device_bytes);
 
+/* ---- packs: several steady solves advanced by one launch of each kernel --------------------------------
+ * No counterpart in the reference (it runs one case per process). A solve is first prepared on the host
+ * (its device layout and byte count, no device memory); a pack concatenates prepared solves that share the
+ * settings the launch sequence depends on (model, scheme, order, time stepping, Nlinear, limiter, gas
+ * model); their flow conditions, CFL schedule, stopping drop and reference length may differ. Cells of a
+ * solve are block aligned and every reduction (norms, time step, coefficients, DPLUR early exit,
+ * convergence stop) is per solve, so a solve's iterations are bit-identical alone and in a pack.
+ * csu_iterate advances every solve of a pack; a converged or failed solve is frozen while the others run.
+ */
+typedef struct csu_prep csu_prep;
+typedef struct csu_solve_info {
+    int iter;        /* iterations done (the solve's own counter)                  */
+    int status;      /* CSU_OK or CSU_ERR_NONFINITE                                 */
+    int done;        /* the residual-drop stop (convDrop) was reached              */
+    int hist_rows;   /* history rows recorded by the last csu_iterate call          */
+    int have_res0;   /* res0 holds the first residual                              */
+    double res0[6];  /* RMS residuals of the solve's first iteration               */
+    double res[6];   /* RMS residuals of its last iteration                         */
+    double coef[4];  /* Cx_p, Cx_v, Cy_p, Cy_v of its last iteration                */
+} csu_solve_info;
+
+int csu_prep_create(const csu_mesh_desc* mesh, const csu_config* cfg, csu_prep** out);
+long long csu_prep_bytes(const csu_prep* p);   /* device bytes the solve needs in a pack   */
+int csu_prep_cells(const csu_prep* p);
+void csu_prep_destroy(csu_prep* p);
+int csu_pack_create(const csu_prep* const* solves, int n, csu_ctx** out);
+int csu_pack_size(csu_ctx* ctx);
+int csu_pack_set_state(csu_ctx* ctx, int k, const double* U);   /* U[nvar][ncells_k], reference order */
+int csu_pack_get_state(csu_ctx* ctx, int k, double* U);
+int csu_pack_info(csu_ctx* ctx, int k, csu_solve_info* info);
+int csu_pack_history(csu_ctx* ctx, int k, double* hist, int max_rows, int* rows);
+int csu_pack_transfer(csu_ctx* from, int k_from, csu_ctx* to, int k_to);
+
 const char* csu_last_error(void);
 const char* csu_strerror(int status);
 
