@@ -47,7 +47,8 @@ class Config(C.Structure):
         ("pin", C.c_double * 7), ("uin", C.c_double * 6), ("mach_inf", C.c_double), ("inlet_p", C.c_double),
         ("inlet_t", C.c_double), ("sst_l", C.c_double), ("k_factor", C.c_double), ("o_factor", C.c_double),
         ("o_wall_factor", C.c_double), ("implicit_fp32", C.c_int), ("implicit_local_dt", C.c_int),
-        ("cfl_ramp_iters", C.c_int), ("cfl_max", C.c_double), ("conv_drop", C.c_double)]
+        ("cfl_ramp_iters", C.c_int), ("cfl_max", C.c_double), ("conv_drop", C.c_double),
+                ("iter_cap", C.c_int)]
 
 
 class MeshDesc(C.Structure):
@@ -108,6 +109,15 @@ def lib():
         L.csu_pack_info.argtypes = [vp, C.c_int, C.POINTER(SolveInfo)]
         L.csu_pack_history.argtypes = [vp, C.c_int, vp, C.c_int, ip]
         L.csu_pack_transfer.argtypes = [vp, C.c_int, vp, C.c_int]
+        L.csu_srv_create.argtypes = [C.POINTER(SrvConfig), C.POINTER(vp)]
+        L.csu_srv_submit.argtypes = [vp, C.POINTER(MeshDesc), C.POINTER(Config), vp, C.c_int,
+                                     C.POINTER(C.c_longlong)]
+        L.csu_srv_step.argtypes = [vp, ip, ip]
+        L.csu_srv_info.argtypes = [vp, C.c_longlong, C.POINTER(SrvInfo)]
+        L.csu_srv_take.argtypes = [vp, C.c_longlong, vp]
+        L.csu_srv_totals.argtypes = [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
+        L.csu_srv_destroy.argtypes = [vp]
+        L.csu_srv_destroy.restype = None
         _lib = L
     return _lib
 
@@ -115,6 +125,18 @@ def lib():
 class SolveInfo(C.Structure):
     _fields_ = [("iter", C.c_int), ("status", C.c_int), ("done", C.c_int), ("hist_rows", C.c_int),
                 ("have_res0", C.c_int), ("res0", C.c_double * 6), ("res", C.c_double * 6), ("coef", C.c_double * 4)]
+
+
+class SrvConfig(C.Structure):
+    _fields_ = [("budget_bytes", C.c_longlong), ("iters_per_step", C.c_int), ("max_pack", C.c_int)]
+
+
+class SrvInfo(C.Structure):
+    _fields_ = [("state", C.c_int), ("iters", C.c_int), ("n_cells", C.c_int), ("drop", C.c_double),
+                ("t_submit", C.c_double), ("t_start", C.c_double), ("t_end", C.c_double)]
+
+
+SRV_STATES = {0: "queued", 1: "running", 2: "converged", 3: "failed", 4: "maxiter"}
 
 
 def _check(st):
@@ -358,6 +380,56 @@ class Pack:
     def close(self):
         if getattr(self, "_h", None) and _lib is not None:
             _lib.csu_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+
+class Server:
+    """Continuous batching of steady solves (csu_srv_*): submit requests as they arrive, call step() in a loop."""
+
+    def __init__(self, budget_bytes, iters_per_step=16, max_pack=0):
+        cfg = SrvConfig(int(budget_bytes), int(iters_per_step), int(max_pack))
+        h = C.c_void_p()
+        _check(lib().csu_srv_create(C.byref(cfg), C.byref(h)))
+        self._h = h
+        self._shape = {}
+
+    def submit(self, case, config=None, state=None, max_iters=100000):
+        cfg = config if config is not None else case.config
+        U = np.ascontiguousarray(case.initial_state() if state is None else state, dtype=np.float64)
+        i = C.c_longlong()
+        _check(lib().csu_srv_submit(self._h, C.byref(case.desc), C.byref(cfg), _ptr(U), int(max_iters),
+                                    C.byref(i)))
+        self._shape[i.value] = (cfg.nvar, case.n_cells)
+        return i.value
+
+    def step(self):
+        r, q = C.c_int(), C.c_int()
+        _check(lib().csu_srv_step(self._h, C.byref(r), C.byref(q)))
+        return r.value, q.value
+
+    def info(self, rid):
+        i = SrvInfo()
+        _check(lib().csu_srv_info(self._h, rid, C.byref(i)))
+        return {"state": SRV_STATES[i.state], "iters": i.iters, "n_cells": i.n_cells, "drop": i.drop,
+                "t_submit": i.t_submit, "t_start": i.t_start, "t_end": i.t_end}
+
+    def take(self, rid):
+        U = np.zeros(self._shape[rid])
+        _check(lib().csu_srv_take(self._h, rid, _ptr(U)))
+        del self._shape[rid]
+        return U
+
+    def totals(self):
+        a, b, c = C.c_longlong(), C.c_longlong(), C.c_longlong()
+        _check(lib().csu_srv_totals(self._h, C.byref(a), C.byref(b), C.byref(c)))
+        return {"solve_iterations": a.value, "cell_updates": b.value, "used_bytes": c.value}
+
+    def close(self):
+        if getattr(self, "_h", None) and _lib is not None:
+            _lib.csu_srv_destroy(self._h)
             self._h = None
 
     def __del__(self):

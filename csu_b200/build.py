@@ -21,7 +21,7 @@ LIB = os.path.join(LIB_DIR, "libcsu_b200.so")
 EXE = os.path.join(BIN_DIR, "csu")
 
 HOST_SOURCES = ["host/input.c", "host/su2.c", "host/case.c", "host/layout.c", "host/driver.c"]
-CUDA_SOURCES = ["cuda/capi.cu", "cuda/noalloc.cu"]
+CUDA_SOURCES = ["cuda/capi.cu", "cuda/noalloc.cu", "cuda/serve.cu"]
 EXE_SOURCES = ["host/main.c"]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")

@@ -37,6 +37,7 @@ struct csu_ctx {
     csu_layout L;
     Prm prm;                 // parameters of solve 0 (the only one outside packs)
     int nsolve = 1;
+    bool is_pack = false;    // made by csu_pack_create (even with one solve): solves keep their own counters
     std::vector<Prm> prms;   // per solve, mirrored at d_prm
     Prm* d_prm = nullptr;
     double* hist = nullptr;  // nsolve blocks of hist_cap rows
@@ -362,6 +363,7 @@ static void fill_params_from(const csu_config& c, const csu_layout& L, Prm& p)
     p.visc = (c.laminar || c.sa || c.sst) ? 1 : 0;
     p.visc_blazek = c.visc_blazek;
     p.conv_tol = c.conv_drop;
+    p.iter_cap = c.iter_cap;
     p.blk32 = c.implicit_fp32;
     p.implicit_local_dt = c.implicit_local_dt;
     p.cfl_ramp_iters = c.cfl_ramp_iters;
@@ -558,7 +560,7 @@ static int solve_state_io(csu_ctx* x, int k, double* U, bool put)
 {
     const int nck = x->ncs[k], o = x->cell0[k], NC = x->L.nc, nv = x->nv;
     // a pack keeps each solve's renumbering (its concatenated layout has none); a one-solve context its own
-    const int* n2o = x->n2o.empty() ? x->L.cell_new2old : x->n2o[k].data();
+    const int* n2o = x->is_pack ? x->n2o[k].data() : x->L.cell_new2old;
     std::vector<double4> u4(nck);
     std::vector<double> ux((size_t)(nv - 4) * nck + 1);
     if (put) {
@@ -600,7 +602,7 @@ static int solve_state_io(csu_ctx* x, int k, double* U, bool put)
 extern "C" int csu_set_state(csu_ctx* x, const double* U)
 {
     if (!x || !U) return CSU_ERR_INPUT;
-    if (!x->n2o.empty()) {
+    if (x->is_pack) {
         csu_set_error("csu_set_state: a pack holds its solves separately (use csu_pack_set_state)");
         return CSU_ERR_STATE;
     }
@@ -610,7 +612,7 @@ extern "C" int csu_set_state(csu_ctx* x, const double* U)
 extern "C" int csu_get_state(csu_ctx* x, double* U)
 {
     if (!x || !U) return CSU_ERR_INPUT;
-    if (!x->n2o.empty()) {
+    if (x->is_pack) {
         csu_set_error("csu_get_state: a pack holds its solves separately (use csu_pack_get_state)");
         return CSU_ERR_STATE;
     }
@@ -824,7 +826,7 @@ static int run_iterations(csu_ctx* x, int n, int it0, Scalars* out)
 {
     int st;
     if ((st = ensure_hist(x, n))) return st;
-    if (!x->prepared && x->nsolve == 1) {
+    if (!x->prepared && !x->is_pack) {
         if ((st = reset_scalars(x, it0))) return st;
     } else {
         // keep the device step state, restart the history rows (and, for one solve, the loop counter;
@@ -833,7 +835,7 @@ static int run_iterations(csu_ctx* x, int n, int it0, Scalars* out)
         if ((st = read_scalars_n(x, hs.data(), x->nsolve))) return st;
         for (Scalars& h : hs) {
             h.hist_row = 0;
-            if (x->nsolve == 1) h.iter = it0;
+            if (!x->is_pack) h.iter = it0;
             h.steps = 0;
         }
         if ((st = write_scalars_n(x, hs.data(), x->nsolve))) return st;
@@ -870,7 +872,7 @@ extern "C" int csu_iterate_ex(csu_ctx* x, int n, int it0, double* hist, int* n_d
     int st = run_iterations(x, n, it0, &h);
     if (!st && n_done) *n_done = h.steps;
     if (st) return st;
-    if (x->nsolve > 1) return CSU_OK; // per-solve results: csu_pack_info, csu_pack_history
+    if (x->is_pack) return CSU_OK; // per-solve results: csu_pack_info, csu_pack_history
     if (hist) {
         int rows = h.hist_row < n ? h.hist_row : n;
         CK(cudaMemcpy(hist, x->hist, sizeof(double) * (size_t)rows * (x->nv + 4), cudaMemcpyDeviceToHost));
@@ -947,7 +949,7 @@ extern "C" int csu_residual(csu_ctx* x, double* R)
 extern "C" int csu_dump(csu_ctx* x, int what, double* out)
 {
     if (!x || !out) return CSU_ERR_INPUT;
-    if (!x->n2o.empty() && what != CSU_DUMP_LSQ_X87) {
+    if (x->is_pack && what != CSU_DUMP_LSQ_X87) {
         csu_set_error("csu_dump: views in reference order are per solve and not available for packs");
         return CSU_ERR_STATE;
     }
@@ -1223,6 +1225,7 @@ extern "C" int csu_pack_create(const csu_prep* const* solves, int n, csu_ctx** o
     x->nv = solves[0]->nv;
     x->cfg = solves[0]->cfg;
     x->nsolve = n;
+    x->is_pack = true;
     std::vector<const csu_layout*> parts(n);
     for (int k = 0; k < n; k++) parts[k] = &solves[k]->L;
     x->cell0.resize(n);

@@ -38,6 +38,7 @@ struct Prm {
     SstK sst_k;         // SST constants (sstInit)
     double tmax;        // tube end time
     double conv_tol;    // stop when res[0] <= conv_tol * res0[0] (0: never)
+    int iter_cap;       // freeze the solve (done = 2) once its counter reaches this (0: never)
     int cell0;          // first cell of this solve (packs: cells [cell0, cell0 + nc), block aligned)
     int blk0, nblk;     // its cell blocks (residual-norm partial sums)
     int wall0, nwall;   // its wall faces in the wall-coefficient array

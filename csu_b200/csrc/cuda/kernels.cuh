@@ -1201,6 +1201,7 @@ __global__ void __launch_bounds__(BLOCK) k_finalize(const Prm* __restrict__ P, c
             if (sc->stop_after) sc->done = 1;
         }
         if (p.conv_tol > 0 && sc->res[0] <= p.conv_tol * sc->res0[0]) sc->done = 1;
+        else if (p.iter_cap > 0 && sc->iter >= p.iter_cap) sc->done = 2;
         for (int k = 0; k < MAX_SWEEPS; k++) sc->sweep_max[k] = 0ULL;
     }
     if (mode == 2 && !sc->fresh) {

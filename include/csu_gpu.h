@@ -85,6 +85,7 @@ typedef struct csu_config {
                                 (keywords CFLramp, CFLmax)                                              */
     double cfl_max;
     double conv_drop;        /* stop once res[0] <= conv_drop * res[0] of the first iteration (convDrop) */
+    int iter_cap;            /* packs: freeze a solve after this many iterations (iterCap; 0: none)     */
 } csu_config;
 
 /*
@@ -243,7 +244,7 @@ typedef struct csu_prep csu_prep;
 typedef struct csu_solve_info {
     int iter;        /* iterations done (the solve's own counter)                  */
     int status;      /* CSU_OK or CSU_ERR_NONFINITE                                 */
-    int done;        /* the residual-drop stop (convDrop) was reached              */
+    int done;        /* 1: the residual-drop stop (convDrop) was reached; 2: iterCap */
     int hist_rows;   /* history rows recorded by the last csu_iterate call          */
     int have_res0;   /* res0 holds the first residual                              */
     double res0[6];  /* RMS residuals of the solve's first iteration               */
@@ -262,6 +263,42 @@ int csu_pack_get_state(csu_ctx* ctx, int k, double* U);
 int csu_pack_info(csu_ctx* ctx, int k, csu_solve_info* info);
 int csu_pack_history(csu_ctx* ctx, int k, double* hist, int max_rows, int* rows);
 int csu_pack_transfer(csu_ctx* from, int k_from, csu_ctx* to, int k_to);
+
+/* ---- serving: continuous batching of steady solves on one GPU ------------------------------------------
+ * No counterpart in the reference. Requests queue on submission; every csu_srv_step retires converged /
+ * failed / capped solves, admits queued requests (first fit, arrival order) while their device bytes
+ * (csu_prep_bytes) fit the budget, rebuilds the packs whose membership changed (continuing solves move with
+ * their iteration state, so each result is the same as the solve alone) and advances every pack by
+ * iters_per_step iterations. Each request stops at its configuration's convDrop (csu_config.conv_drop) or
+ * after max_iters iterations. Times are seconds since csu_srv_create (host clock).
+ */
+#define CSU_SRV_QUEUED 0
+#define CSU_SRV_RUNNING 1
+#define CSU_SRV_CONVERGED 2
+#define CSU_SRV_FAILED 3
+#define CSU_SRV_MAXITER 4
+typedef struct csu_srv csu_srv;
+typedef struct csu_srv_config {
+    long long budget_bytes;  /* device bytes the running solves may take                      */
+    int iters_per_step;      /* iterations per csu_srv_step (a multiple of 8 replays graphs)   */
+    int max_pack;            /* most solves per pack (0: no limit)                             */
+} csu_srv_config;
+typedef struct csu_srv_request_info {
+    int state;               /* CSU_SRV_*                                                      */
+    int iters;               /* iterations done                                                */
+    int n_cells;
+    double drop;             /* RMS rho-residual / its first value                             */
+    double t_submit, t_start, t_end;
+} csu_srv_request_info;
+
+int csu_srv_create(const csu_srv_config* cfg, csu_srv** out);
+int csu_srv_submit(csu_srv* s, const csu_mesh_desc* mesh, const csu_config* cfg, const double* U0, int max_iters,
+                   long long* id);
+int csu_srv_step(csu_srv* s, int* n_running, int* n_queued);
+int csu_srv_info(csu_srv* s, long long id, csu_srv_request_info* out);
+int csu_srv_take(csu_srv* s, long long id, double* U);      /* final state (reference order); forgets it */
+int csu_srv_totals(csu_srv* s, long long* solve_iterations, long long* cell_updates, long long* used_bytes);
+void csu_srv_destroy(csu_srv* s);
 
 const char* csu_last_error(void);
 const char* csu_strerror(int status);
