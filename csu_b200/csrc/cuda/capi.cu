@@ -1274,6 +1274,31 @@ extern "C" int csu_pack_get_state(csu_ctx* x, int k, double* U)
     return solve_state_io(x, k, U, false);
 }
 
+static void solve_info_from(const csu_ctx* x, const Scalars& h, csu_solve_info* info)
+{
+    memset(info, 0, sizeof(*info));
+    info->iter = h.iter;
+    info->status = h.status;
+    info->done = h.done;
+    info->hist_rows = h.hist_row < h.hist_cap ? h.hist_row : h.hist_cap;
+    info->have_res0 = h.have_res0;
+    for (int v = 0; v < x->nv; v++) {
+        info->res0[v] = h.res0[v];
+        info->res[v] = h.res[v];
+    }
+    for (int v = 0; v < 4; v++) info->coef[v] = h.coef[v];
+}
+
+extern "C" int csu_pack_infos(csu_ctx* x, csu_solve_info* infos)
+{
+    if (!x || !infos) return CSU_ERR_INPUT;
+    std::vector<Scalars> hs(x->nsolve);
+    int st = read_scalars_n(x, hs.data(), x->nsolve);
+    if (st) return st;
+    for (int k = 0; k < x->nsolve; k++) solve_info_from(x, hs[k], infos + k);
+    return CSU_OK;
+}
+
 extern "C" int csu_pack_info(csu_ctx* x, int k, csu_solve_info* info)
 {
     if (!x || !info || k < 0 || k >= x->nsolve) return CSU_ERR_INPUT;

@@ -3,12 +3,13 @@
 //
 // Requests (a mesh, a configuration with its stopping drop, an initial state) queue on arrival. Each call of
 // csu_srv_step (the caller's persistent request loop):
-//   1. retires the running solves that converged (residual drop), failed (non-finite) or reached their
-//      iteration cap, and keeps their final states until taken;
-//   2. admits queued requests, first fit in arrival order, while their device bytes fit the budget;
-//   3. rebuilds the pack of every class whose membership changed: the continuing solves move with their
-//      full iteration state (csu_pack_transfer), so a solve's iterations are the same whatever joins or
-//      leaves; the new members start from their initial states;
+//   1. reads back the solves that converged (residual drop), failed (non-finite) or reached their
+//      iteration cap; they stay frozen in their pack until its next rebuild;
+//   2. admits queued requests, first fit in arrival order, while their device bytes fit the budget, into a
+//      class whose pack may be rebuilt now (at most every `rebuild_steps` steps, or when it is empty);
+//   3. rebuilds the packs with admissions: running solves move with their full iteration state
+//      (csu_pack_transfer), so a solve's iterations are the same whatever joins or leaves; finished ones are
+//      dropped and their bytes released; the new members start from their initial states;
 //   4. advances every pack by `iters_per_step` iterations (CUDA graphs; one launch per kernel per
 //      iteration for all members).
 // A class is the set of settings a pack shares (model, scheme, order, time stepping, ...); requests of
@@ -33,8 +34,9 @@ struct Req;
 struct Group {
     csu_config key;
     csu_ctx* pack = nullptr;
-    std::vector<Req*> members; // in pack order
-    bool dirty = false;
+    std::vector<Req*> members; // in pack order (finished ones stay frozen until the next rebuild)
+    std::vector<Req*> pending; // admitted, joining at the next rebuild
+    int steps_since = 0;       // steps since the pack was built
 };
 
 struct Req {
@@ -49,7 +51,8 @@ struct Req {
     int iters = 0;
     double drop = 0;
     long long bytes = 0;
-    Group* group = nullptr;
+    Group* group = nullptr;   // the group whose pack holds it (frozen there once finished)
+    bool taken = false;       // result taken while still frozen in a pack: freed at the rebuild
 };
 
 bool same_class(const csu_config& a, const csu_config& b)
@@ -126,35 +129,28 @@ extern "C" int csu_srv_submit(csu_srv* s, const csu_mesh_desc* mesh, const csu_c
     return CSU_OK;
 }
 
+// Marks the pack's solves that finished (converged, failed, capped): their states are read back; they
+// stay frozen in the pack (holding their bytes) until the next rebuild drops them.
 static int retire(csu_srv* s, Group* g)
 {
     if (!g->pack) return CSU_OK;
-    std::vector<Req*> keep;
+    std::vector<csu_solve_info> infos(g->members.size());
+    int st = csu_pack_infos(g->pack, infos.data());
+    if (st) return st;
     for (size_t k = 0; k < g->members.size(); k++) {
         Req* r = g->members[k];
-        csu_solve_info info;
-        int st = csu_pack_info(g->pack, (int)k, &info);
-        if (st) return st;
+        if (r->state != CSU_SRV_RUNNING) continue;
+        const csu_solve_info& info = infos[k];
         r->iters = info.iter;
         r->drop = info.have_res0 && info.res0[0] > 0 ? info.res[0] / info.res0[0] : 1.0;
         int fin = info.status ? CSU_SRV_FAILED
                   : info.done == 1 ? CSU_SRV_CONVERGED
                   : (info.done == 2 || info.iter >= r->max_iters) ? CSU_SRV_MAXITER : 0;
-        if (!fin) {
-            keep.push_back(r);
-            continue;
-        }
+        if (!fin) continue;
         if ((st = csu_pack_get_state(g->pack, (int)k, r->U.data()))) return st;
         r->state = fin;
         r->t_end = s->now();
-        r->group = nullptr;
-        s->used -= r->bytes;
-        csu_prep_destroy(r->prep);
-        r->prep = nullptr;
-        g->dirty = true;
     }
-    // the retired solves' slots are released when the pack is rebuilt
-    if (g->dirty) g->members = keep;
     return CSU_OK;
 }
 
@@ -168,32 +164,53 @@ static Group* group_for(csu_srv* s, const csu_config& c)
     return g;
 }
 
-static int rebuild(csu_srv* s, Group* g, const std::vector<Req*>& old_members)
+static int active(const Group* g)
+{
+    int n = 0;
+    for (const Req* r : g->members) n += r->state == CSU_SRV_RUNNING;
+    return n;
+}
+
+// New pack of the group's running solves (moved with their iteration state) and the admitted ones (from
+// their initial states); finished solves are dropped and their bytes released.
+static int rebuild(csu_srv* s, Group* g)
 {
     csu_ctx* old = g->pack;
+    std::vector<Req*> old_members = g->members;
+    std::vector<Req*> next;
+    for (Req* r : old_members) {
+        if (r->state == CSU_SRV_RUNNING) next.push_back(r);
+        else {
+            s->used -= r->bytes;
+            if (r->prep) csu_prep_destroy(r->prep);
+            r->prep = nullptr;
+            r->group = nullptr;
+            if (r->taken) delete r;
+        }
+    }
+    for (Req* r : g->pending) next.push_back(r);
+    g->pending.clear();
+    g->members = next;
     g->pack = nullptr;
+    g->steps_since = 0;
     int st = CSU_OK;
-    if (!g->members.empty()) {
+    if (!next.empty()) {
         std::vector<const csu_prep*> preps;
-        for (Req* r : g->members) preps.push_back(r->prep);
+        for (Req* r : next) preps.push_back(r->prep);
         if ((st = csu_pack_create(preps.data(), (int)preps.size(), &g->pack))) {
             if (old) csu_destroy(old);
             return st;
         }
-        for (size_t k = 0; k < g->members.size(); k++) {
-            Req* r = g->members[k];
+        for (size_t k = 0; k < next.size() && !st; k++) {
+            Req* r = next[k];
             auto it = std::find(old_members.begin(), old_members.end(), r);
-            if (old && it != old_members.end()) {
+            if (old && it != old_members.end())
                 st = csu_pack_transfer(old, (int)(it - old_members.begin()), g->pack, (int)k);
-            } else {
+            else
                 st = csu_pack_set_state(g->pack, (int)k, r->U.data());
-            }
-            if (st) break;
         }
     }
     if (old) csu_destroy(old);
-    g->dirty = false;
-    (void)s;
     return st;
 }
 
@@ -201,39 +218,45 @@ extern "C" int csu_srv_step(csu_srv* s, int* n_running, int* n_queued)
 {
     if (!s) return CSU_ERR_INPUT;
     int st;
-    // 1. retire (member lists of the old packs are kept for the transfers below)
-    std::map<Group*, std::vector<Req*>> before;
-    for (Group* g : s->groups) {
-        before[g] = g->members;
+    // 1. finished solves
+    for (Group* g : s->groups)
         if ((st = retire(s, g))) return st;
-    }
-    // 2. admit, first fit in arrival order
+    // 2. admit, first fit in arrival order, into groups whose pack may be rebuilt now
+    const int every = s->cfg.rebuild_steps > 1 ? s->cfg.rebuild_steps : 1;
     for (auto it = s->queue.begin(); it != s->queue.end();) {
         Req* r = *it;
         Group* g = group_for(s, r->cfg);
-        if (s->used + r->bytes <= s->cfg.budget_bytes && (int)g->members.size() < s->cfg.max_pack) {
+        bool window = !g->pack || active(g) == 0 || g->steps_since >= every;
+        int size = active(g) + (int)g->pending.size();
+        if (window && s->used + r->bytes <= s->cfg.budget_bytes && size < s->cfg.max_pack) {
             s->used += r->bytes;
             r->state = CSU_SRV_RUNNING;
             r->t_start = s->now();
             r->group = g;
-            g->members.push_back(r);
-            g->dirty = true;
+            g->pending.push_back(r);
             it = s->queue.erase(it);
         } else {
             ++it;
         }
     }
-    // 3. rebuild changed packs
-    for (Group* g : s->groups)
-        if (g->dirty && (st = rebuild(s, g, before[g]))) return st;
+    // 3. rebuild packs with admissions, and packs whose solves all finished
+    for (Group* g : s->groups) {
+        bool idle = g->pack && active(g) == 0;
+        if (!g->pending.empty() || idle)
+            if ((st = rebuild(s, g))) return st;
+    }
     // 4. advance
     int running = 0;
     for (Group* g : s->groups) {
         if (!g->pack) continue;
         if ((st = csu_iterate(g->pack, s->cfg.iters_per_step, 0, nullptr))) return st;
-        running += (int)g->members.size();
-        for (Req* r : g->members) s->cell_updates += (long long)r->nc * s->cfg.iters_per_step;
-        s->iterations += (long long)g->members.size() * s->cfg.iters_per_step;
+        g->steps_since++;
+        for (Req* r : g->members) {
+            if (r->state != CSU_SRV_RUNNING) continue;
+            running++;
+            s->cell_updates += (long long)r->nc * s->cfg.iters_per_step;
+            s->iterations += s->cfg.iters_per_step;
+        }
     }
     if (n_running) *n_running = running;
     if (n_queued) *n_queued = (int)s->queue.size();
@@ -270,8 +293,9 @@ extern "C" int csu_srv_take(csu_srv* s, long long id, double* U)
         return CSU_ERR_STATE;
     }
     if (U) memcpy(U, r->U.data(), sizeof(double) * r->U.size());
-    delete r;
     s->reqs.erase(it);
+    if (r->group) r->taken = true; // still frozen in a pack: released when the pack is rebuilt
+    else delete r;
     return CSU_OK;
 }
 
@@ -288,6 +312,11 @@ extern "C" void csu_srv_destroy(csu_srv* s)
 {
     if (!s) return;
     for (Group* g : s->groups) {
+        for (Req* r : g->members)
+            if (r->taken) {
+                if (r->prep) csu_prep_destroy(r->prep);
+                delete r;
+            }
         if (g->pack) csu_destroy(g->pack);
         delete g;
     }

@@ -233,6 +233,14 @@ static int build_neighbours(csu_mesh* m)
         m->bface[3 * b + 2] = best;
         m->cell_nei[4 * best + cnt[best]++] = -(1 + b);
     }
+    /* every edge needs a neighbour: the reference would follow a dangling pointer (an edge with neither a
+       second cell nor a boundary marker); refuse such meshes */
+    for (int c = 0; c < nc; c++)
+        if (cnt[c] != m->cell_npts[c]) {
+            csu_set_error("mesh: cell %d has %d edges but %d neighbours (an edge with neither a second cell nor "
+                          "a boundary marker)", c, m->cell_npts[c], cnt[c]);
+            goto fail;
+        }
     free(cnt); free(pstart); free(plist);
     return CSU_OK;
 fail:

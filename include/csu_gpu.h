@@ -261,6 +261,7 @@ int csu_pack_size(csu_ctx* ctx);
 int csu_pack_set_state(csu_ctx* ctx, int k, const double* U);   /* U[nvar][ncells_k], reference order */
 int csu_pack_get_state(csu_ctx* ctx, int k, double* U);
 int csu_pack_info(csu_ctx* ctx, int k, csu_solve_info* info);
+int csu_pack_infos(csu_ctx* ctx, csu_solve_info* infos);        /* all solves, one device read */
 int csu_pack_history(csu_ctx* ctx, int k, double* hist, int max_rows, int* rows);
 int csu_pack_transfer(csu_ctx* from, int k_from, csu_ctx* to, int k_to);
 
@@ -282,6 +283,9 @@ typedef struct csu_srv_config {
     long long budget_bytes;  /* device bytes the running solves may take                      */
     int iters_per_step;      /* iterations per csu_srv_step (a multiple of 8 replays graphs)   */
     int max_pack;            /* most solves per pack (0: no limit)                             */
+    int rebuild_steps;       /* admit into a running pack at most every this many steps (a pack
+                                rebuild re-uploads its meshes; finished solves stay frozen in the
+                                pack until the next rebuild); 0 or 1: every step                  */
 } csu_srv_config;
 typedef struct csu_srv_request_info {
     int state;               /* CSU_SRV_*                                                      */
