@@ -109,6 +109,7 @@ def lib():
         L.csu_pack_info.argtypes = [vp, C.c_int, C.POINTER(SolveInfo)]
         L.csu_pack_history.argtypes = [vp, C.c_int, vp, C.c_int, ip]
         L.csu_pack_transfer.argtypes = [vp, C.c_int, vp, C.c_int]
+        L.csu_pack_rebuild.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(vp), C.c_int, C.POINTER(vp)]
         L.csu_srv_create.argtypes = [C.POINTER(SrvConfig), C.POINTER(vp)]
         L.csu_srv_submit.argtypes = [vp, C.POINTER(MeshDesc), C.POINTER(Config), vp, C.c_int,
                                      C.POINTER(C.c_longlong)]
@@ -116,6 +117,7 @@ def lib():
         L.csu_srv_info.argtypes = [vp, C.c_longlong, C.POINTER(SrvInfo)]
         L.csu_srv_take.argtypes = [vp, C.c_longlong, vp]
         L.csu_srv_totals.argtypes = [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
+        L.csu_srv_times.argtypes = [vp, dp, dp, dp, ip]
         L.csu_srv_destroy.argtypes = [vp]
         L.csu_srv_destroy.restype = None
         _lib = L
@@ -370,6 +372,21 @@ class Pack:
         _check(lib().csu_pack_history(self._h, k, _ptr(out), min(rows, max_rows), C.byref(n)))
         return out[:n.value]
 
+    def rebuilt(self, keep, preps):
+        """A new pack of `preps`; member k is member keep[k] of this pack (mesh and iteration state moved on
+        the device) when keep[k] >= 0, else starts from its prep's state."""
+        new = Pack.__new__(Pack)
+        new.preps = list(preps)
+        km = (C.c_int * len(new.preps))(*[int(v) for v in keep])
+        arr = (C.c_void_p * len(new.preps))(*[p._h.value for p in new.preps])
+        h = C.c_void_p()
+        _check(lib().csu_pack_rebuild(self._h, km, arr, len(new.preps), C.byref(h)))
+        new._h = h
+        for k, p in enumerate(new.preps):
+            if keep[k] < 0:
+                new.set_state(k, p.state)
+        return new
+
     def transfer_from(self, other, k_other, k):
         _check(lib().csu_pack_transfer(other._h, k_other, self._h, k))
 
@@ -426,7 +443,10 @@ class Server:
     def totals(self):
         a, b, c = C.c_longlong(), C.c_longlong(), C.c_longlong()
         _check(lib().csu_srv_totals(self._h, C.byref(a), C.byref(b), C.byref(c)))
-        return {"solve_iterations": a.value, "cell_updates": b.value, "used_bytes": c.value}
+        r, i, p, n = C.c_double(), C.c_double(), C.c_double(), C.c_int()
+        _check(lib().csu_srv_times(self._h, C.byref(r), C.byref(i), C.byref(p), C.byref(n)))
+        return {"solve_iterations": a.value, "cell_updates": b.value, "used_bytes": c.value,
+                "rebuild_s": r.value, "iterate_s": i.value, "poll_s": p.value, "rebuilds": n.value}
 
     def close(self):
         if getattr(self, "_h", None) and _lib is not None:

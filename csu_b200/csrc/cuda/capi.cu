@@ -6,6 +6,7 @@
 #include <string.h>
 #include <math.h>
 #include <vector>
+#include <algorithm>
 #include "csu_gpu.h"
 #include "kernels.cuh"
 
@@ -38,6 +39,7 @@ struct csu_ctx {
     Prm prm;                 // parameters of solve 0 (the only one outside packs)
     int nsolve = 1;
     bool is_pack = false;    // made by csu_pack_create (even with one solve): solves keep their own counters
+    bool pack_wall_d = false;// packs: the solves carry wall distances (SA, SST)
     std::vector<Prm> prms;   // per solve, mirrored at d_prm
     Prm* d_prm = nullptr;
     double* hist = nullptr;  // nsolve blocks of hist_cap rows
@@ -137,7 +139,7 @@ static void plan(csu_ctx* x, Arena& a)
     m.omega = carve<double>(a, nc);
     m.sxh = carve<double>(a, nc);
     m.syh = carve<double>(a, nc);
-    m.wall_d = x->L.wall_d ? carve<double>(a, nc) : nullptr;
+    m.wall_d = (x->is_pack ? x->pack_wall_d : x->L.wall_d != nullptr) ? carve<double>(a, nc) : nullptr;
     m.dslat = carve<double>(a, nc);
     m.fe = carve<int2>(a, nf);
     m.fn = carve<double2>(a, nf);
@@ -489,7 +491,7 @@ static int ctx_setup(csu_ctx* x)
     x->gb_c = (x->L.nc + BLOCK - 1) / BLOCK;
     x->gb_fi = (x->L.nf + BLOCK - 1) / BLOCK;
     x->gb_fb = (x->L.nb + BLOCK - 1) / BLOCK;
-    if ((st = upload_mesh(x))) return st;
+    if (!x->is_pack && (st = upload_mesh(x))) return st; // packs: pack_build fills the mesh rows
     x->prm = x->prms[0];
     if ((st = upload_prm(x)) || (st = reset_scalars(x, 0))) return st;
     switch (x->cfg.stages) {
@@ -1199,64 +1201,6 @@ extern "C" void csu_prep_destroy(csu_prep* p)
     delete p;
 }
 
-extern "C" int csu_pack_create(const csu_prep* const* solves, int n, csu_ctx** out)
-{
-    if (!out) return CSU_ERR_INPUT;
-    *out = nullptr;
-    if (!solves || n < 1) {
-        csu_set_error("csu_pack_create: no solves");
-        return CSU_ERR_INPUT;
-    }
-    for (int k = 0; k < n; k++) {
-        if (!solves[k]) return CSU_ERR_INPUT;
-        if (!same_structure(solves[0]->cfg, solves[k]->cfg)) {
-            csu_set_error("csu_pack_create: solve %d differs from solve 0 in a setting a pack shares (model, "
-                          "scheme, order, time stepping, ...)", k);
-            return CSU_ERR_INPUT;
-        }
-    }
-    int ndev = 0;
-    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
-        csu_set_error("csu_pack_create: no CUDA device");
-        return CSU_ERR_NO_DEVICE;
-    }
-    csu_ctx* x = new csu_ctx();
-    x->model = solves[0]->model;
-    x->nv = solves[0]->nv;
-    x->cfg = solves[0]->cfg;
-    x->nsolve = n;
-    x->is_pack = true;
-    std::vector<const csu_layout*> parts(n);
-    for (int k = 0; k < n; k++) parts[k] = &solves[k]->L;
-    x->cell0.resize(n);
-    x->face0.resize(n);
-    x->bface0.resize(n);
-    int st = csu_layout_concat(parts.data(), n, BLOCK, &x->L, x->cell0.data(), x->face0.data(), x->bface0.data());
-    if (st) {
-        delete x;
-        csu_set_error("csu_pack_create: layouts could not be packed");
-        return st;
-    }
-    x->prms.resize(n);
-    x->ncs.resize(n);
-    x->n2o.resize(n);
-    for (int k = 0; k < n; k++) {
-        const csu_layout& L = solves[k]->L;
-        fill_params_from(solves[k]->cfg, L, x->prms[k]);
-        x->prms[k].cell0 = x->cell0[k];
-        x->prms[k].blk0 = x->cell0[k] / BLOCK;
-        x->prms[k].nblk = (L.nc + BLOCK - 1) / BLOCK;
-        x->ncs[k] = L.nc;
-        x->n2o[k].assign(L.cell_new2old, L.cell_new2old + L.nc);
-    }
-    if ((st = ctx_setup(x))) {
-        csu_destroy(x);
-        return st;
-    }
-    *out = x;
-    return CSU_OK;
-}
-
 extern "C" int csu_pack_size(csu_ctx* x)
 {
     return x ? x->nsolve : 0;
@@ -1377,4 +1321,323 @@ extern "C" int csu_pack_transfer(csu_ctx* from, int kf, csu_ctx* to, int kt)
     CK(cudaMemcpy(to->st.sc + kt, &ht, sizeof(Scalars), cudaMemcpyHostToDevice));
     to->prepared = 0;
     return CSU_OK;
+}
+
+// ------------------------------------------------------------------------------------------------ pack assembly
+// A pack's mesh arrays are its solves' arrays side by side. Building a pack copies each solve's rows into
+// place -- from the host layout of a new solve, or device to device from the pack that held it before --
+// and then re-bases the index-valued entries (cells, ghost and face codes, wall ranks) on the new offsets.
+// No concatenated host layout is built, and a rebuild uploads only the solves that are new.
+
+namespace {
+
+enum { SEG_CELL = 0, SEG_CELL4, SEG_FACE, SEG_BFACE };
+
+struct SegArr {
+    char* dev;
+    size_t es;
+    int kind;
+};
+
+// Where a solve's rows lie: cells [c0, c0 + nc), faces [f0, ...), boundary faces [b0, ...) of a pack with
+// NC cells (stride of [slot][cell] arrays, ghost base) and NF interior faces (boundary flux base); w0 is the
+// solve's first wall rank.
+struct SegGeo {
+    int c0, nc, f0, nf, b0, nb, NC, NF, w0;
+};
+
+} // namespace
+
+static std::vector<SegArr> seg_arrays(csu_ctx* x)
+{
+    Mesh& m = x->mesh;
+    auto P = [](const void* p) { return (char*)const_cast<void*>(p); };
+    std::vector<SegArr> v = {
+        {P(m.npts), 4, SEG_CELL}, {P(m.nint), 4, SEG_CELL}, {P(m.nslot), 4, SEG_CELL},
+        {P(m.nei), 4, SEG_CELL4}, {P(m.wx), 8, SEG_CELL4}, {P(m.wy), 8, SEG_CELL4},
+        {P(m.ldx), 8, SEG_CELL4}, {P(m.ldy), 8, SEG_CELL4}, {P(m.lm), 8, SEG_CELL4},
+        {P(m.les), 4, SEG_CELL4}, {P(m.lrv), 8, SEG_CELL}, {P(m.lq), 16, SEG_CELL4},
+        {P(m.ex), 8, SEG_CELL4}, {P(m.ey), 8, SEG_CELL4}, {P(m.fslot), 4, SEG_CELL4},
+        {P(m.omega), 8, SEG_CELL}, {P(m.sxh), 8, SEG_CELL}, {P(m.syh), 8, SEG_CELL},
+        {P(m.dslat), 8, SEG_CELL}, {P(m.color), 4, SEG_CELL},
+        {P(m.fe), 8, SEG_FACE}, {P(m.fn), 16, SEG_FACE}, {P(m.fds), 8, SEG_FACE}, {P(m.r0), 16, SEG_FACE},
+        {P(m.r1), 16, SEG_FACE}, {P(m.fd), 16, SEG_FACE}, {P(m.fL), 8, SEG_FACE},
+        {P(m.bown), 4, SEG_BFACE}, {P(m.bflag), 4, SEG_BFACE}, {P(m.bold), 4, SEG_BFACE},
+        {P(m.bn), 16, SEG_BFACE}, {P(m.bds), 8, SEG_BFACE}, {P(m.bd), 16, SEG_BFACE}, {P(m.bL), 8, SEG_BFACE},
+        {P(m.bun), 16, SEG_BFACE}, {P(m.bds2), 8, SEG_BFACE}, {P(x->d_wall_rank), 4, SEG_BFACE}};
+    if (m.wall_d) v.push_back({P(m.wall_d), 8, SEG_CELL});
+    return v;
+}
+
+// Walls of one solve in reference (marker-major) order: rank per boundary face, -1 elsewhere.
+static int local_wall_ranks(const csu_layout& L, int* rank)
+{
+    std::vector<int> by_old(L.nb, -1);
+    for (int b = 0; b < L.nb; b++) by_old[L.bold[b]] = b;
+    int r = 0;
+    for (int b = 0; b < L.nb; b++) rank[b] = -1;
+    for (int o = 0; o < L.nb; o++) {
+        int b = by_old[o];
+        if (L.bflag[b] == CSU_BC_WALL || L.bflag[b] == CSU_BC_WALLT) rank[b] = r++;
+    }
+    return r;
+}
+
+// The same arrays of one solve's host layout, in seg_arrays order (device formats built in `keep`).
+static std::vector<const void*> seg_host(const csu_layout& L, std::vector<std::vector<char>>& keep)
+{
+    const int nf = L.nf, nb = L.nb;
+    auto pairs = [&](const double* a, const double* b, int n) {
+        keep.emplace_back((size_t)n * sizeof(double2) + 1);
+        double2* d = (double2*)keep.back().data();
+        for (int i = 0; i < n; i++) d[i] = make_double2(a[i], b[i]);
+        return (const void*)d;
+    };
+    keep.emplace_back((size_t)nf * sizeof(int2) + 1);
+    int2* fe = (int2*)keep.back().data();
+    for (int f = 0; f < nf; f++) fe[f] = make_int2(L.fe0[f], L.fe1[f]);
+    keep.emplace_back((size_t)nb * sizeof(int) + 1);
+    int* rank = (int*)keep.back().data();
+    local_wall_ranks(L, rank);
+    std::vector<const void*> v = {
+        L.npts, L.nint, L.nslot, L.nei, L.wx, L.wy, L.ldx, L.ldy, L.lm, L.les, L.lrv, L.lq, L.ex, L.ey, L.fslot,
+        L.omega, L.sxh, L.syh, L.dslat, L.color,
+        fe, pairs(L.fdsx, L.fdsy, nf), L.fds, pairs(L.r0x, L.r0y, nf), pairs(L.r1x, L.r1y, nf),
+        pairs(L.fdx, L.fdy, nf), L.fdist,
+        L.bown, L.bflag, L.bold, pairs(L.bdsx, L.bdsy, nb), L.bds, pairs(L.bdx, L.bdy, nb), L.bL,
+        pairs(L.bunx, L.buny, nb), L.bds2, rank};
+    if (L.wall_d) v.push_back(L.wall_d);
+    return v;
+}
+
+// Re-bases the index-valued rows of one solve from geometry S (where they were written) to D.
+__global__ void k_seg_fix(Mesh m, int* wall_rank, SegGeo S, SegGeo D)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int dc = D.c0 - S.c0;
+    if (t < D.nc) {
+        int c = D.c0 + t;
+        int* nei = const_cast<int*>(m.nei);
+        int* fs = const_cast<int*>(m.fslot);
+        for (int j = 0; j < 4; j++) {
+            size_t o = (size_t)j * D.NC + c;
+            int v = nei[o];
+            nei[o] = v < S.NC ? v + dc : v - S.NC - S.b0 + D.NC + D.b0;
+            int f = fs[o];
+            if (f != 0) {
+                int a = (f < 0 ? -f : f) - 1;
+                a = a < S.NF ? a - S.f0 + D.f0 : a - S.NF - S.b0 + D.NF + D.b0;
+                fs[o] = f < 0 ? -(a + 1) : a + 1;
+            }
+        }
+    }
+    if (t < D.nf) {
+        int2* fe = const_cast<int2*>(m.fe);
+        int2 e = fe[D.f0 + t];
+        fe[D.f0 + t] = make_int2(e.x + dc, e.y + dc);
+    }
+    if (t < D.nb) {
+        int* bown = const_cast<int*>(m.bown);
+        bown[D.b0 + t] += dc;
+        int r = wall_rank[D.b0 + t];
+        if (r >= 0) wall_rank[D.b0 + t] = r - S.w0 + D.w0;
+    }
+}
+
+static SegGeo seg_geo(const csu_ctx* x, int k)
+{
+    SegGeo g;
+    g.c0 = x->cell0[k];
+    g.nc = x->ncs[k];
+    g.f0 = x->face0[k];
+    g.nf = x->prms[k].nf;
+    g.b0 = x->bface0[k];
+    g.nb = x->prms[k].nb;
+    g.NC = x->L.nc;
+    g.NF = x->L.nf;
+    g.w0 = x->prms[k].wall0;
+    return g;
+}
+
+// Copies solve k's mesh rows into x: device to device from solve ks of `src`, or from `L` (src null).
+static int seg_fill(csu_ctx* x, int k, const csu_layout* L, csu_ctx* src, int ks)
+{
+    SegGeo D = seg_geo(x, k), S;
+    std::vector<SegArr> dst = seg_arrays(x);
+    if (src) {
+        S = seg_geo(src, ks);
+        std::vector<SegArr> from = seg_arrays(src);
+        if (from.size() != dst.size()) return CSU_ERR_INPUT;
+        for (size_t a = 0; a < dst.size(); a++) {
+            const size_t es = dst[a].es;
+            auto cp = [&](size_t so, size_t dof, size_t n) {
+                return cudaMemcpyAsync(dst[a].dev + dof * es, from[a].dev + so * es, n * es,
+                                       cudaMemcpyDeviceToDevice, x->stream);
+            };
+            switch (dst[a].kind) {
+            case SEG_CELL: CK(cp(S.c0, D.c0, D.nc)); break;
+            case SEG_CELL4:
+                for (int j = 0; j < 4; j++) CK(cp((size_t)j * S.NC + S.c0, (size_t)j * D.NC + D.c0, D.nc));
+                break;
+            case SEG_FACE: if (D.nf) CK(cp(S.f0, D.f0, D.nf)); break;
+            default: if (D.nb) CK(cp(S.b0, D.b0, D.nb)); break;
+            }
+        }
+    } else {
+        S = {0, L->nc, 0, L->nf, 0, L->nb, L->nc, L->nf, 0};
+        std::vector<std::vector<char>> keep;
+        std::vector<const void*> from = seg_host(*L, keep);
+        if (from.size() != dst.size()) return CSU_ERR_INPUT;
+        CK(cudaStreamSynchronize(x->stream));
+        for (size_t a = 0; a < dst.size(); a++) {
+            const size_t es = dst[a].es;
+            const char* h = (const char*)from[a];
+            auto up = [&](size_t so, size_t dof, size_t n) {
+                return cudaMemcpy(dst[a].dev + dof * es, h + so * es, n * es, cudaMemcpyHostToDevice);
+            };
+            switch (dst[a].kind) {
+            case SEG_CELL: CK(up(0, D.c0, D.nc)); break;
+            case SEG_CELL4:
+                for (int j = 0; j < 4; j++) CK(up((size_t)j * S.NC, (size_t)j * D.NC + D.c0, D.nc));
+                break;
+            case SEG_FACE: if (D.nf) CK(up(0, D.f0, D.nf)); break;
+            default: if (D.nb) CK(up(0, D.b0, D.nb)); break;
+            }
+        }
+    }
+    int nt = std::max(D.nc, std::max(D.nf, D.nb));
+    if (nt > 0) k_seg_fix<<<(nt + BLOCK - 1) / BLOCK, BLOCK, 0, x->stream>>>(x->mesh, x->d_wall_rank, S, D);
+    CK(cudaGetLastError());
+    return CSU_OK;
+}
+
+// A pack of `solves`; with `old`, solve k with keep[k] >= 0 comes from solve keep[k] of `old` (its mesh rows
+// and iteration state copied on the device), the others from their host layouts (initial state to be set).
+static int pack_build(const char* who, const csu_prep* const* solves, int n, csu_ctx* old, const int* keep,
+                      csu_ctx** out)
+{
+    if (!out) return CSU_ERR_INPUT;
+    *out = nullptr;
+    if (!solves || n < 1) {
+        csu_set_error("%s: no solves", who);
+        return CSU_ERR_INPUT;
+    }
+    for (int k = 0; k < n; k++) {
+        if (!solves[k]) return CSU_ERR_INPUT;
+        if (!same_structure(solves[0]->cfg, solves[k]->cfg)) {
+            csu_set_error("%s: solve %d differs from solve 0 in a setting a pack shares (model, scheme, order, "
+                          "time stepping, ...)", who, k);
+            return CSU_ERR_INPUT;
+        }
+        if (old && keep && keep[k] >= 0) {
+            if (keep[k] >= old->nsolve || old->ncs[keep[k]] != solves[k]->L.nc ||
+                !same_structure(old->cfg, solves[k]->cfg)) {
+                csu_set_error("%s: solve %d does not match solve %d of the old pack", who, k, keep[k]);
+                return CSU_ERR_INPUT;
+            }
+        }
+    }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        csu_set_error("%s: no CUDA device", who);
+        return CSU_ERR_NO_DEVICE;
+    }
+    csu_ctx* x = new csu_ctx();
+    x->model = solves[0]->model;
+    x->nv = solves[0]->nv;
+    x->cfg = solves[0]->cfg;
+    x->nsolve = n;
+    x->is_pack = true;
+    x->pack_wall_d = solves[0]->L.wall_d != nullptr;
+    x->cell0.resize(n);
+    x->face0.resize(n);
+    x->bface0.resize(n);
+    x->prms.resize(n);
+    x->ncs.resize(n);
+    x->n2o.resize(n);
+    memset(&x->L, 0, sizeof(x->L));
+    int NC = 0, NF = 0, NB = 0, K = 0, walls = 0;
+    std::vector<int> rank;
+    for (int k = 0; k < n; k++) {
+        const csu_layout& L = solves[k]->L;
+        x->cell0[k] = NC;
+        x->face0[k] = NF;
+        x->bface0[k] = NB;
+        NC += (L.nc + BLOCK - 1) / BLOCK * BLOCK;
+        NF += L.nf;
+        NB += L.nb;
+        if (L.ncolors > K) K = L.ncolors;
+        Prm& p = x->prms[k];
+        fill_params_from(solves[k]->cfg, L, p);
+        p.cell0 = x->cell0[k];
+        p.blk0 = x->cell0[k] / BLOCK;
+        p.nblk = (L.nc + BLOCK - 1) / BLOCK;
+        rank.resize(L.nb + 1);
+        p.wall0 = walls;
+        p.nwall = local_wall_ranks(L, rank.data());
+        walls += p.nwall;
+        x->ncs[k] = L.nc;
+        x->n2o[k].assign(L.cell_new2old, L.cell_new2old + L.nc);
+    }
+    x->L.nc = NC;
+    x->L.nf = NF;
+    x->L.nb = NB;
+    x->nwall = walls;
+    // colour lists over the pack (LU-SGS): same-colour cells of all solves together, ascending
+    x->L.ncolors = K;
+    x->L.color_start = (int*)calloc(K + 1, sizeof(int));
+    std::vector<int> color_cells(NC > 0 ? NC : 1);
+    for (int k = 0; k < n; k++)
+        for (int c = 0; c < solves[k]->L.nc; c++) x->L.color_start[solves[k]->L.color[c] + 1]++;
+    for (int q = 0; q < K; q++) x->L.color_start[q + 1] += x->L.color_start[q];
+    {
+        std::vector<int> fill(x->L.color_start, x->L.color_start + K + 1);
+        for (int k = 0; k < n; k++)
+            for (int c = 0; c < solves[k]->L.nc; c++) color_cells[fill[solves[k]->L.color[c]]++] = x->cell0[k] + c;
+    }
+    int st = ctx_setup(x);
+    // mesh rows, solve maps and colour lists
+    for (int k = 0; k < n && !st; k++) {
+        bool kept = old && keep && keep[k] >= 0;
+        st = kept ? seg_fill(x, k, nullptr, old, keep[k]) : seg_fill(x, k, &solves[k]->L, nullptr, 0);
+    }
+    if (!st) {
+        int nblk = (NC + BLOCK - 1) / BLOCK;
+        std::vector<int> bs(nblk, 0), cs(NC, 0);
+        for (int k = 0; k < n; k++) {
+            int c1 = k + 1 < n ? x->cell0[k + 1] : NC;
+            for (int c = x->cell0[k]; c < c1; c++) cs[c] = k;
+            for (int b = x->cell0[k] / BLOCK; b < (c1 + BLOCK - 1) / BLOCK; b++) bs[b] = k;
+        }
+        cudaError_t e = cudaStreamSynchronize(x->stream);
+        if (e == cudaSuccess && n > 1) e = cudaMemcpy(const_cast<int*>(x->st.bsolve), bs.data(), sizeof(int) * nblk, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && n > 1) e = cudaMemcpy(const_cast<int*>(x->st.csolve), cs.data(), sizeof(int) * NC, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(const_cast<int*>(x->mesh.color_cells), color_cells.data(), sizeof(int) * NC,
+                           cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) st = cuda_fail(e, "pack maps");
+    }
+    // iteration state of the kept solves
+    for (int k = 0; k < n && !st; k++)
+        if (old && keep && keep[k] >= 0) st = csu_pack_transfer(old, keep[k], x, k);
+    if (st) {
+        csu_destroy(x);
+        return st;
+    }
+    *out = x;
+    return CSU_OK;
+}
+
+extern "C" int csu_pack_create(const csu_prep* const* solves, int n, csu_ctx** out)
+{
+    return pack_build("csu_pack_create", solves, n, nullptr, nullptr, out);
+}
+
+extern "C" int csu_pack_rebuild(csu_ctx* old, const int* keep, const csu_prep* const* solves, int n, csu_ctx** out)
+{
+    if (!old || !old->is_pack || !keep) {
+        csu_set_error("csu_pack_rebuild: an old pack and the keep map are required");
+        return CSU_ERR_INPUT;
+    }
+    return pack_build("csu_pack_rebuild", solves, n, old, keep, out);
 }

@@ -77,6 +77,8 @@ struct csu_srv {
     long long next_id = 1;
     long long iterations = 0;      // solve-iterations run (sum over members)
     long long cell_updates = 0;    // cells x iterations run
+    double t_rebuild = 0, t_iterate = 0, t_poll = 0; // host seconds in the phases of csu_srv_step
+    int rebuilds = 0;
     std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
 
     double now() const
@@ -197,18 +199,20 @@ static int rebuild(csu_srv* s, Group* g)
     if (!next.empty()) {
         std::vector<const csu_prep*> preps;
         for (Req* r : next) preps.push_back(r->prep);
-        if ((st = csu_pack_create(preps.data(), (int)preps.size(), &g->pack))) {
+        // running solves move on the device (mesh rows and iteration state); new ones are uploaded
+        std::vector<int> keep(next.size(), -1);
+        for (size_t k = 0; k < next.size(); k++) {
+            auto it = std::find(old_members.begin(), old_members.end(), next[k]);
+            if (old && it != old_members.end()) keep[k] = (int)(it - old_members.begin());
+        }
+        st = old ? csu_pack_rebuild(old, keep.data(), preps.data(), (int)preps.size(), &g->pack)
+                 : csu_pack_create(preps.data(), (int)preps.size(), &g->pack);
+        if (st) {
             if (old) csu_destroy(old);
             return st;
         }
-        for (size_t k = 0; k < next.size() && !st; k++) {
-            Req* r = next[k];
-            auto it = std::find(old_members.begin(), old_members.end(), r);
-            if (old && it != old_members.end())
-                st = csu_pack_transfer(old, (int)(it - old_members.begin()), g->pack, (int)k);
-            else
-                st = csu_pack_set_state(g->pack, (int)k, r->U.data());
-        }
+        for (size_t k = 0; k < next.size() && !st; k++)
+            if (keep[k] < 0) st = csu_pack_set_state(g->pack, (int)k, next[k]->U.data());
     }
     if (old) csu_destroy(old);
     return st;
@@ -219,8 +223,10 @@ extern "C" int csu_srv_step(csu_srv* s, int* n_running, int* n_queued)
     if (!s) return CSU_ERR_INPUT;
     int st;
     // 1. finished solves
+    double t = s->now();
     for (Group* g : s->groups)
         if ((st = retire(s, g))) return st;
+    s->t_poll += s->now() - t;
     // 2. admit, first fit in arrival order, into groups whose pack may be rebuilt now
     const int every = s->cfg.rebuild_steps > 1 ? s->cfg.rebuild_steps : 1;
     for (auto it = s->queue.begin(); it != s->queue.end();) {
@@ -240,12 +246,17 @@ extern "C" int csu_srv_step(csu_srv* s, int* n_running, int* n_queued)
         }
     }
     // 3. rebuild packs with admissions, and packs whose solves all finished
+    t = s->now();
     for (Group* g : s->groups) {
         bool idle = g->pack && active(g) == 0;
-        if (!g->pending.empty() || idle)
+        if (!g->pending.empty() || idle) {
             if ((st = rebuild(s, g))) return st;
+            s->rebuilds++;
+        }
     }
+    s->t_rebuild += s->now() - t;
     // 4. advance
+    t = s->now();
     int running = 0;
     for (Group* g : s->groups) {
         if (!g->pack) continue;
@@ -258,6 +269,7 @@ extern "C" int csu_srv_step(csu_srv* s, int* n_running, int* n_queued)
             s->iterations += s->cfg.iters_per_step;
         }
     }
+    s->t_iterate += s->now() - t;
     if (n_running) *n_running = running;
     if (n_queued) *n_queued = (int)s->queue.size();
     return CSU_OK;
@@ -296,6 +308,16 @@ extern "C" int csu_srv_take(csu_srv* s, long long id, double* U)
     s->reqs.erase(it);
     if (r->group) r->taken = true; // still frozen in a pack: released when the pack is rebuilt
     else delete r;
+    return CSU_OK;
+}
+
+extern "C" int csu_srv_times(csu_srv* s, double* rebuild_s, double* iterate_s, double* poll_s, int* rebuilds)
+{
+    if (!s) return CSU_ERR_INPUT;
+    if (rebuild_s) *rebuild_s = s->t_rebuild;
+    if (iterate_s) *iterate_s = s->t_iterate;
+    if (poll_s) *poll_s = s->t_poll;
+    if (rebuilds) *rebuilds = s->rebuilds;
     return CSU_OK;
 }
 

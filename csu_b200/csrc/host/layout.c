@@ -404,146 +404,3 @@ int csu_layout_build(const csu_mesh_desc* m, int axi, csu_layout* L)
     free(cy);
     return CSU_OK;
 }
-
-/*
- * Packs: the layouts of several solves concatenated into one, so that every kernel launch advances all of
- * them. Solve k owns cells [cell0[k], cell0[k] + nc_k), with cell0 a multiple of `align` (the cell block
- * size: every block then holds cells of one solve; the rest of a solve's last block is padding that no
- * face references), interior faces [face0[k], ...) and boundary faces [bface0[k], ...). Indices are
- * offset; the neighbour and face-slot codes are re-based on the pack's totals. Renumbering permutations
- * stay with the parts (the pack's are NULL).
- */
-int csu_layout_concat(const csu_layout* const* parts, int n, int align, csu_layout* P, int* cell0, int* face0,
-                      int* bface0)
-{
-    memset(P, 0, sizeof(*P));
-    int NC = 0, NF = 0, NB = 0, K = 0, wd = parts[0]->wall_d != NULL;
-    for (int k = 0; k < n; k++) {
-        const csu_layout* L = parts[k];
-        cell0[k] = NC;
-        face0[k] = NF;
-        bface0[k] = NB;
-        NC += (L->nc + align - 1) / align * align;
-        NF += L->nf;
-        NB += L->nb;
-        if (L->ncolors > K) K = L->ncolors;
-        if ((L->wall_d != NULL) != wd) return CSU_ERR_INPUT;
-        if (L->nv != parts[0]->nv) return CSU_ERR_INPUT;
-        if (L->max_npts > P->max_npts) P->max_npts = L->max_npts;
-        if (L->vol_max > P->vol_max) P->vol_max = L->vol_max;
-    }
-    P->nc = NC;
-    P->nf = NF;
-    P->nb = NB;
-    P->nv = parts[0]->nv;
-    size_t c4 = (size_t)4 * NC;
-#define PALLOC(ptr, count)                                                                                    \
-    do {                                                                                                      \
-        (ptr) = calloc((count) > 0 ? (count) : 1, sizeof(*(ptr)));                                            \
-        if (!(ptr)) goto oom;                                                                                 \
-    } while (0)
-    PALLOC(P->npts, NC); PALLOC(P->nint, NC); PALLOC(P->nslot, NC); PALLOC(P->nei, c4);
-    PALLOC(P->wx, c4); PALLOC(P->wy, c4); PALLOC(P->ldx, c4); PALLOC(P->ldy, c4);
-    PALLOC(P->lm, c4); PALLOC(P->les, c4); PALLOC(P->lrv, NC); PALLOC(P->lq, 2 * c4);
-    PALLOC(P->ex, c4); PALLOC(P->ey, c4); PALLOC(P->fslot, c4);
-    PALLOC(P->omega, NC); PALLOC(P->sxh, NC); PALLOC(P->syh, NC); PALLOC(P->xc, NC); PALLOC(P->yc, NC);
-    if (wd) PALLOC(P->wall_d, NC);
-    PALLOC(P->dslat, NC);
-    PALLOC(P->fe0, NF); PALLOC(P->fe1, NF); PALLOC(P->fdsx, NF); PALLOC(P->fdsy, NF); PALLOC(P->fds, NF);
-    PALLOC(P->r0x, NF); PALLOC(P->r0y, NF); PALLOC(P->r1x, NF); PALLOC(P->r1y, NF); PALLOC(P->fdist, NF);
-    PALLOC(P->fdx, NF); PALLOC(P->fdy, NF);
-    PALLOC(P->bown, NB); PALLOC(P->bflag, NB); PALLOC(P->bold, NB); PALLOC(P->bdsx, NB); PALLOC(P->bdsy, NB);
-    PALLOC(P->bds, NB); PALLOC(P->bmx, NB); PALLOC(P->bmy, NB); PALLOC(P->bdx, NB); PALLOC(P->bdy, NB);
-    PALLOC(P->bL, NB); PALLOC(P->bunx, NB); PALLOC(P->buny, NB); PALLOC(P->bds2, NB);
-    PALLOC(P->color, NC); PALLOC(P->color_start, K + 1); PALLOC(P->color_cells, NC);
-#undef PALLOC
-    for (int c = 0; c < NC; c++) P->omega[c] = 1.0; /* padding */
-    for (int k = 0; k < n; k++) {
-        const csu_layout* L = parts[k];
-        const int nc = L->nc, nf = L->nf, nb = L->nb, o = cell0[k], fo = face0[k], bo = bface0[k];
-        for (int c = 0; c < nc; c++) {
-            int d = o + c;
-            P->npts[d] = L->npts[c];
-            P->nint[d] = L->nint[c];
-            P->nslot[d] = L->nslot[c];
-            P->lrv[d] = L->lrv[c];
-            P->omega[d] = L->omega[c];
-            P->sxh[d] = L->sxh[c];
-            P->syh[d] = L->syh[c];
-            P->xc[d] = L->xc[c];
-            P->yc[d] = L->yc[c];
-            if (wd) P->wall_d[d] = L->wall_d[c];
-            P->dslat[d] = L->dslat[c];
-            P->color[d] = L->color[c];
-            for (int j = 0; j < 4; j++) {
-                size_t s = (size_t)j * nc + c, t = (size_t)j * NC + d;
-                int v = L->nei[s];
-                P->nei[t] = v < nc ? v + o : NC + bo + (v - nc);
-                int f = L->fslot[s];
-                if (f == 0) P->fslot[t] = 0;
-                else if (f < 0) P->fslot[t] = f - fo;
-                else if (f <= nf) P->fslot[t] = f + fo;
-                else P->fslot[t] = NF + bo + (f - nf);
-                P->wx[t] = L->wx[s];
-                P->wy[t] = L->wy[s];
-                P->ldx[t] = L->ldx[s];
-                P->ldy[t] = L->ldy[s];
-                P->lm[t] = L->lm[s];
-                P->les[t] = L->les[s];
-                P->lq[2 * t] = L->lq[2 * s];
-                P->lq[2 * t + 1] = L->lq[2 * s + 1];
-                P->ex[t] = L->ex[s];
-                P->ey[t] = L->ey[s];
-            }
-        }
-        for (int f = 0; f < nf; f++) {
-            int d = fo + f;
-            P->fe0[d] = L->fe0[f] + o;
-            P->fe1[d] = L->fe1[f] + o;
-            P->fdsx[d] = L->fdsx[f];
-            P->fdsy[d] = L->fdsy[f];
-            P->fds[d] = L->fds[f];
-            P->r0x[d] = L->r0x[f];
-            P->r0y[d] = L->r0y[f];
-            P->r1x[d] = L->r1x[f];
-            P->r1y[d] = L->r1y[f];
-            P->fdist[d] = L->fdist[f];
-            P->fdx[d] = L->fdx[f];
-            P->fdy[d] = L->fdy[f];
-        }
-        for (int b = 0; b < nb; b++) {
-            int d = bo + b;
-            P->bown[d] = L->bown[b] + o;
-            P->bflag[d] = L->bflag[b];
-            P->bold[d] = L->bold[b];
-            P->bdsx[d] = L->bdsx[b];
-            P->bdsy[d] = L->bdsy[b];
-            P->bds[d] = L->bds[b];
-            P->bmx[d] = L->bmx[b];
-            P->bmy[d] = L->bmy[b];
-            P->bdx[d] = L->bdx[b];
-            P->bdy[d] = L->bdy[b];
-            P->bL[d] = L->bL[b];
-            P->bunx[d] = L->bunx[b];
-            P->buny[d] = L->buny[b];
-            P->bds2[d] = L->bds2[b];
-        }
-    }
-    /* colour lists over the pack: same-colour cells of all solves together, ascending */
-    P->ncolors = K;
-    for (int k = 0; k < n; k++)
-        for (int c = 0; c < parts[k]->nc; c++) P->color_start[parts[k]->color[c] + 1]++;
-    for (int q = 0; q < K; q++) P->color_start[q + 1] += P->color_start[q];
-    {
-        int* fill = malloc(sizeof(int) * (K + 1));
-        if (!fill) goto oom;
-        memcpy(fill, P->color_start, sizeof(int) * (K + 1));
-        for (int k = 0; k < n; k++)
-            for (int c = 0; c < parts[k]->nc; c++) P->color_cells[fill[parts[k]->color[c]]++] = cell0[k] + c;
-        free(fill);
-    }
-    return CSU_OK;
-oom:
-    csu_layout_free(P);
-    return CSU_ERR_OOM;
-}

@@ -88,8 +88,6 @@ typedef struct csu_layout {
 
 int csu_layout_build(const csu_mesh_desc* m, int axi, csu_layout* L);
 void csu_layout_free(csu_layout* L);
-int csu_layout_concat(const csu_layout* const* parts, int n, int align, csu_layout* P, int* cell0, int* face0,
-                      int* bface0);
 
 #ifdef __cplusplus
 }

@@ -117,9 +117,10 @@ def run_batched(reqs, cases, max_iters, budget_bytes, iters_per_step=16, rebuild
         states.append(srv.take(ids[k]))
         res.append({"finish": info["t_end"], "iters": info["iters"], "converged": info["state"] == "converged",
                     "failed": info["state"] == "failed"})
-    cu = srv.totals()["cell_updates"]
+    tot = srv.totals()
     srv.close()
-    return res, states, cu, makespan
+    run_batched.last_totals = tot
+    return res, states, tot["cell_updates"], makespan
 
 
 def summarize(reqs, res, cu, makespan):
@@ -152,6 +153,7 @@ def run(n=40, seed=0, rate=5.0, cells_lo=1e4, cells_hi=2e5, drop=1e-8, max_iters
     batched = summarize(reqs, br, bcu, bt)
     both = [k for k in range(n) if pr[k]["converged"] and br[k]["converged"]]
     diff = state_difference([bs[k] for k in both], [ps[k] for k in both]) if both else None
+    batched["server"] = getattr(run_batched, "last_totals", None)
     return {"plain": plain, "batched": batched, "state_diff_rel": diff,
             "iters_plain": [x["iters"] for x in pr], "iters_batched": [x["iters"] for x in br],
             "workload": {"requests": n, "seed": seed, "rate_per_s": rate, "cells": [cells_lo, cells_hi],

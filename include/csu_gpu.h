@@ -264,6 +264,10 @@ int csu_pack_info(csu_ctx* ctx, int k, csu_solve_info* info);
 int csu_pack_infos(csu_ctx* ctx, csu_solve_info* infos);        /* all solves, one device read */
 int csu_pack_history(csu_ctx* ctx, int k, double* hist, int max_rows, int* rows);
 int csu_pack_transfer(csu_ctx* from, int k_from, csu_ctx* to, int k_to);
+/* A new pack of `solves` in which solve k, when keep[k] >= 0, is solve keep[k] of `old` (mesh rows and
+ * iteration state copied on the device, nothing re-uploaded); the others come from their host layouts and
+ * need csu_pack_set_state. `old` is left unchanged (destroy it afterwards). */
+int csu_pack_rebuild(csu_ctx* old, const int* keep, const csu_prep* const* solves, int n, csu_ctx** out);
 
 /* ---- serving: continuous batching of steady solves on one GPU ------------------------------------------
  * No counterpart in the reference. Requests queue on submission; every csu_srv_step retires converged /
@@ -302,6 +306,8 @@ int csu_srv_step(csu_srv* s, int* n_running, int* n_queued);
 int csu_srv_info(csu_srv* s, long long id, csu_srv_request_info* out);
 int csu_srv_take(csu_srv* s, long long id, double* U);      /* final state (reference order); forgets it */
 int csu_srv_totals(csu_srv* s, long long* solve_iterations, long long* cell_updates, long long* used_bytes);
+/* host seconds spent rebuilding packs, iterating and polling, and the number of rebuilds */
+int csu_srv_times(csu_srv* s, double* rebuild_s, double* iterate_s, double* poll_s, int* rebuilds);
 void csu_srv_destroy(csu_srv* s);
 
 const char* csu_last_error(void);

@@ -87,3 +87,22 @@ def test_pack_transfer_continues_solve(native):
     hb, Ub = _alone(b[0], b[1], 18)
     assert np.array_equal(second.get_state(0), Ub)
     second.close()
+
+
+def test_pack_rebuild_moves_solves_on_device(native):
+    """A rebuilt pack (new member first, kept members reordered) continues the kept solves bit-identically
+    and runs the new one as it would alone."""
+    import csu_b200
+    a, b, c = MEMBERS[0], MEMBERS[1], MEMBERS[2]
+    pa, pb, pc = (csu_b200.Prep(_case(*m)) for m in (a, b, c))
+    first = csu_b200.Pack([pa, pb])
+    first.iterate(10)
+    second = first.rebuilt([-1, 1, 0], [pc, pb, pa])
+    first.close()
+    second.iterate(20)
+    for k, (m, n, skip) in enumerate([(c, 20, 0), (b, 30, 10), (a, 30, 10)]):
+        hist, U = _alone(m[0], m[1], n)
+        assert second.info(k)["iter"] == n
+        assert np.array_equal(second.get_state(k), U), m[0]
+        assert np.array_equal(second.history(k), hist[skip:]), m[0]
+    second.close()
