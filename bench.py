@@ -169,6 +169,26 @@ def reference_arm(args, rank):
     return 0
 
 
+def serve_arm(args):
+    """Serving stream (csu_b200.servebench): requests of four geometry families arriving as a Poisson stream,
+    served by the continuous-batching server (packs, FP32 DPLUR blocks) and by the plain FP64 path one solve
+    at a time; metric: converged solves per hour of the batched server."""
+    import torch
+    torch.cuda.set_device(0)
+    from csu_b200 import servebench
+    out = servebench.run(n=args.requests, cells_hi=args.cells_hi)
+    b, p = out["batched"], out["plain"]
+    line = {"metric": "converged solves/hr", "value": b["solves_per_hour"], "unit": "solves/hr", "n_gpus": 1,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64 residual, f32 DPLUR",
+            "data": "synthetic", "config": dict(out["workload"], workload="serving stream"),
+            "p50_s": b["p50_s"], "p99_s": b["p99_s"], "cell_updates_per_s": b["cell_updates_per_s"],
+            "vs_plain_fp64": b["solves_per_hour"] / p["solves_per_hour"] if p["solves_per_hour"] else None,
+            "plain_fp64": p, "batched": b, "state_diff_rel": out["state_diff_rel"],
+            "iters": out["iters_batched"]}
+    print(json.dumps(line))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -176,7 +196,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="csu", choices=["csu", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve", action="store_true",
+                    help="the serving stream instead: batched mixed precision vs plain FP64, one solve at a time")
+    ap.add_argument("--requests", type=int, default=40)
+    ap.add_argument("--cells-hi", type=float, default=2e5)
     args = ap.parse_args()
+    if args.serve:
+        return serve_arm(args)
     args.warmup = max(args.warmup, 3)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
