@@ -26,6 +26,7 @@ struct Arena {
 
 // RK stage coefficients of solverStepRK (solver.c:788-840)
 const double RK1[1] = {1.0};
+const double RK2[2] = {0.5, 1.0}; // extension: midpoint rule (the reference has no 2-stage scheme)
 const double RK3[3] = {0.1481, 0.4, 1.0};
 const double RK4[4] = {0.0833, 0.2069, 0.4265, 1.0};
 const double RK5[5] = {0.0533, 0.1263, 0.2375, 0.4414, 1.0};
@@ -366,6 +367,8 @@ static void fill_params_from(const csu_config& c, const csu_layout& L, Prm& p)
     p.visc_blazek = c.visc_blazek;
     p.conv_tol = c.conv_drop;
     p.iter_cap = c.iter_cap;
+    p.lim_func = c.limiter_func;
+    if (c.gradient == 1) p.lsq_exact = 0; // Green-Gauss weights replace the least-squares weights
     p.blk32 = c.implicit_fp32;
     p.implicit_local_dt = c.implicit_local_dt;
     p.cfl_ramp_iters = c.cfl_ramp_iters;
@@ -446,10 +449,18 @@ static int validate_config(const char* who, const csu_config* cfg, int* model_ou
         csu_set_error("%s: LU-SGS with SST is not available in this engine build", who);
         return CSU_ERR_UNSUPPORTED;
     }
-    if (cfg->time_scheme == CSU_TS_RK && !(cfg->stages == 1 || cfg->stages == 3 || cfg->stages == 4 ||
-                                            cfg->stages == 5)) {
-        csu_set_error("%s: RK with %d stages (the reference implements 1, 3, 4, 5)", who, cfg->stages);
+    if (cfg->time_scheme == CSU_TS_RK && !(cfg->stages >= 1 && cfg->stages <= 5)) {
+        csu_set_error("%s: RK with %d stages (1, 3, 4, 5 as the reference; 2 as an extension)", who, cfg->stages);
         return CSU_ERR_UNSUPPORTED;
+    }
+    if (cfg->limiter_func != 0 && cfg->limiter_func != 1) {
+        csu_set_error("%s: limiterFunc %d (0 Venkatakrishnan, 1 Barth-Jespersen)", who, cfg->limiter_func);
+        return CSU_ERR_INPUT;
+    }
+    if (cfg->gradient != 0 && (cfg->gradient != 1 || cfg->axisymmetric)) {
+        csu_set_error("%s: gradient %d%s (0 least squares, 1 Green-Gauss, planar only)", who, cfg->gradient,
+                      cfg->axisymmetric ? " with axisymmetry" : "");
+        return CSU_ERR_INPUT;
     }
     if (cfg->time_scheme == CSU_TS_DPLUR && (cfg->n_linear < 1 || cfg->n_linear > MAX_SWEEPS)) {
         csu_set_error("%s: Nlinear must be in [1, %d]", who, MAX_SWEEPS);
@@ -459,8 +470,13 @@ static int validate_config(const char* who, const csu_config* cfg, int* model_ou
         csu_set_error("%s: order must be 1 or 2", who);
         return CSU_ERR_INPUT;
     }
-    if (cfg->limiter_type != 0) {
-        csu_set_error("%s: limiter type %d not available in this engine build", who, cfg->limiter_type);
+    if (cfg->limiter_type != 0 && cfg->limiter_type != 1) {
+        csu_set_error("%s: limiter type %d (the reference has types 0 and 1)", who, cfg->limiter_type);
+        return CSU_ERR_INPUT;
+    }
+    if (cfg->limiter_type == 1 && model == 2) {
+        csu_set_error("%s: limiter type 1 with SST (the reference writes past its 5-entry Pmin/Pmax, "
+                      "limiter.c:37-38)", who);
         return CSU_ERR_UNSUPPORTED;
     }
     *model_out = model;
@@ -496,6 +512,7 @@ static int ctx_setup(csu_ctx* x)
     if ((st = upload_prm(x)) || (st = reset_scalars(x, 0))) return st;
     switch (x->cfg.stages) {
     case 1: x->rk = RK1; break;
+    case 2: x->rk = RK2; break;
     case 3: x->rk = RK3; break;
     case 4: x->rk = RK4; break;
     default: x->rk = RK5; break;
@@ -523,6 +540,7 @@ extern "C" int csu_create(const csu_mesh_desc* md, const csu_config* cfg, csu_ct
     x->nv = nv;
     x->cfg = *cfg;
     st = csu_layout_build(md, cfg->axisymmetric, &x->L);
+    if (!st && cfg->gradient == 1) st = csu_layout_green_gauss(&x->L);
     if (st) {
         delete x;
         csu_set_error("csu_create: mesh layout failed (a cell with more than four faces?)");
@@ -654,6 +672,11 @@ static void launch_grad_lsq(csu_ctx* x)
 template <int MODEL>
 static void launch_grad(csu_ctx* x, bool dbg)
 {
+    if (x->cfg.order == 2 && x->cfg.limiter_type == 1) {
+        k_minmax_init<<<x->nsolve, 32, 0, x->stream>>>(x->st);
+        k_minmax<MODEL><<<x->gb_c, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st);
+        x->launches += 2;
+    }
     if (dbg) launch_grad_lsq<MODEL, true>(x);
     else launch_grad_lsq<MODEL, false>(x);
     x->launches++;
@@ -1165,6 +1188,7 @@ extern "C" int csu_prep_create(const csu_mesh_desc* md, const csu_config* cfg, c
     p->model = model;
     p->nv = nv;
     st = csu_layout_build(md, cfg->axisymmetric, &p->L);
+    if (!st && cfg->gradient == 1) st = csu_layout_green_gauss(&p->L);
     if (st) {
         delete p;
         csu_set_error("csu_prep_create: mesh layout failed (a cell with more than four faces?)");

@@ -99,9 +99,8 @@ __device__ __forceinline__ void lsq_consts(const Mesh& m, int nc, int c, X80* K)
 __device__ __forceinline__ double limiter_eps2(const Prm& p, const Scalars* sc, int kk, double aux)
 {
     if (p.limiter_type == 0) return p.pref20[kk] * aux;
-    int mm = kk == 4 ? 5 : kk; // limiter.c:66-70 (SST reads k for both scalars)
-    int sl = mm > 4 ? mm - 1 : mm;
-    double a2 = (ordbits_inv(sc->qmax_bits[sl]) - ordbits_inv(sc->qmin_bits[sl])) * p.lim_k;
+    // type 1 (limiter.c:61-94): ((max - min) K)^2 over the solve's cells, from k_minmax
+    double a2 = (ordbits_inv(sc->qmax_bits[kk]) - ordbits_inv(sc->qmin_bits[kk])) * p.lim_k;
     return a2 * a2;
 }
 
@@ -146,6 +145,50 @@ __device__ __forceinline__ double2 lsq_slot_x87(const Prm& p, const Mesh& m, con
     X80 ny = x80_add(x80_mul(x80_neg(K[1]), XA), x80_mul(K[0], XB));
     atomicAdd(s.lsq_x87, 1ULL);
     return make_double2(x80_to_double(x80_div_pre(nx, K[3], rv)), x80_to_double(x80_div_pre(ny, K[3], rv)));
+}
+
+// ------------------------------------------------------------------------------------------------
+// k_minmax: limiterUpdate type 1 (limiter.c:61-94): the minimum and maximum over the solve's cells of each
+// limited primitive (slot 4 reads P[5], limiter.c:66-70), as order-preserving bits (exact, order-free).
+// k_minmax_init resets them, one block per solve.
+// ------------------------------------------------------------------------------------------------
+__global__ void k_minmax_init(State s)
+{
+    Scalars* sc = s.sc + blockIdx.x;
+    if (threadIdx.x < 6) {
+        sc->qmin_bits[threadIdx.x] = ~0ULL;
+        sc->qmax_bits[threadIdx.x] = 0ULL;
+    }
+}
+
+template <int MODEL>
+__global__ void __launch_bounds__(BLOCK) k_minmax(const Prm* __restrict__ P, const __grid_constant__ Mesh m,
+                                                  const __grid_constant__ State s)
+{
+    constexpr int NV = Model<MODEL>::NV, NP = Model<MODEL>::NP;
+    const int sid = block_solve(s);
+    const Prm& p = P[sid];
+    Scalars* const sc = s.sc + sid;
+    if (halted(sc)) return;
+    const int c = blockIdx.x * BLOCK + threadIdx.x;
+    const bool ok = cell_in(p, c);
+    double W[NP];
+    if (ok) loadP<MODEL>(s, m.nc, c, W);
+#pragma unroll
+    for (int kk = 0; kk < NV; kk++) {
+        double v = ok ? W[kk == 4 ? 5 : kk] : 0.0;
+        const bool use = ok && !isnan(v); // fmin / fmax skip NaN operands (limiter.c:84-85)
+        unsigned long long lo = use ? ordbits(v) : ~0ULL, hi = use ? ordbits(v) : 0ULL;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+            hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+        }
+        if ((threadIdx.x & 31) == 0) {
+            atomicMin(&sc->qmin_bits[kk], lo);
+            atomicMax(&sc->qmax_bits[kk], hi);
+        }
+    }
 }
 
 template <int MODEL, bool DBG, int LSQ>
@@ -352,7 +395,8 @@ __global__ void __launch_bounds__(BLOCK, 2) k_grad(const Prm* __restrict__ P, co
 #pragma unroll
                     for (int kk = 0; kk < NV; kk++) {
                         double d2 = (gx[kk] * exj + gy[kk] * eyj);
-                        double phi0 = limiterV2(P0[slot2p(kk)], qmin[kk], qmax[kk], d2, ee[kk]);
+                        double phi0 = p.lim_func == 1 ? limiterBJ(P0[slot2p(kk)], qmin[kk], qmax[kk], d2)
+                                                      : limiterV2(P0[slot2p(kk)], qmin[kk], qmax[kk], d2, ee[kk]);
                         phi[kk] = j == 0 ? phi0 : fmin(phi[kk], phi0);
                     }
                 }

@@ -484,6 +484,16 @@ __device__ __forceinline__ void bcInlet(const Gas& g, const double* Pa, const do
     }
 }
 
+// limiterBJ (solver.c:1132-1150): Barth-Jespersen, min(1, (Umax - Ui) / d2) -- the minmod limiter function
+// min(1, r) of the ratio of the largest admissible change to the reconstructed one. The reference defines
+// it but never calls it; here it is selected by the limiterFunc extension.
+__host__ __device__ __forceinline__ double limiterBJ(double Ui, double Umin, double Umax, double d2)
+{
+    if (d2 == 0) return 1.0;
+    if (d2 > 0) return fmin(1.0, (Umax - Ui) / d2);
+    return fmin(1.0, (Umin - Ui) / d2);
+}
+
 // boundaryOutlet (boundary.c:53-83)
 __device__ __forceinline__ void bcOutlet(const Gas& g, double pout, const double* Pd, double* Pb, double nx,
                                          double ny)

@@ -341,6 +341,8 @@ static int setup(csu_case* cs, const char* mesh_text, size_t mesh_len, const cha
     c->cfl_max = kw_dbl(kw, "CFLmax", c->cfl);
     c->conv_drop = kw_dbl(kw, "convDrop", 0.0);
     c->iter_cap = kw_int(kw, "iterCap", 0);
+    c->limiter_func = kw_int(kw, "limiterFunc", 0);
+    c->gradient = kw_int(kw, "gradient", 0);
 
     if (c->sa == 1 || c->sst == 1) csu_mesh_wall_distance(&cs->mesh);
 

@@ -404,3 +404,44 @@ int csu_layout_build(const csu_mesh_desc* m, int axi, csu_layout* L)
     free(cy);
     return CSU_OK;
 }
+
+/*
+ * Green-Gauss gradient weights (an extension; the reference uses least squares, solver.c:1031-1074):
+ * grad q_i = (1 / Omega_i) sum_j q_f S_j with the face value q_f = (q_i + q_j) / 2 and outward face vectors
+ * S_j; since sum_j S_j = 0 on a closed planar cell, grad q_i = sum_j (q_j - q_i) S_j / (2 Omega_i), the
+ * same linear form in the neighbour differences as the least-squares weights, which it replaces.
+ */
+int csu_layout_green_gauss(csu_layout* L)
+{
+    const int nc = L->nc, nf = L->nf;
+    for (int c = 0; c < nc; c++) {
+        const double w = 0.5 / L->omega[c];
+        for (int j = 0; j < L->npts[c]; j++) {
+            int n = L->nei[(size_t)j * nc + c];
+            double sx = 0.0, sy = 0.0;
+            int found = 0;
+            if (n >= nc) {
+                int b = n - nc;
+                sx = L->bdsx[b];
+                sy = L->bdsy[b];
+                found = 1;
+            } else {
+                for (int s = 0; s < L->nint[c] && !found; s++) {
+                    int sf = L->fslot[(size_t)s * nc + c];
+                    int f = (sf > 0 ? sf : -sf) - 1;
+                    if (f >= nf) continue;
+                    int other = L->fe0[f] == c ? L->fe1[f] : L->fe0[f];
+                    if (other != n) continue;
+                    double sg = L->fe0[f] == c ? 1.0 : -1.0;
+                    sx = sg * L->fdsx[f];
+                    sy = sg * L->fdsy[f];
+                    found = 1;
+                }
+            }
+            if (!found) return CSU_ERR_INPUT;
+            L->wx[(size_t)j * nc + c] = sx * w;
+            L->wy[(size_t)j * nc + c] = sy * w;
+        }
+    }
+    return CSU_OK;
+}

@@ -88,6 +88,7 @@ typedef struct csu_layout {
 
 int csu_layout_build(const csu_mesh_desc* m, int axi, csu_layout* L);
 void csu_layout_free(csu_layout* L);
+int csu_layout_green_gauss(csu_layout* L);
 
 #ifdef __cplusplus
 }

@@ -86,6 +86,8 @@ typedef struct csu_config {
     double cfl_max;
     double conv_drop;        /* stop once res[0] <= conv_drop * res[0] of the first iteration (convDrop) */
     int iter_cap;            /* packs: freeze a solve after this many iterations (iterCap; 0: none)     */
+    int limiter_func;        /* limiterFunc: 0 Venkatakrishnan (reference), 1 Barth-Jespersen / minmod  */
+    int gradient;            /* gradient: 0 least squares (reference), 1 Green-Gauss                    */
 } csu_config;
 
 /*

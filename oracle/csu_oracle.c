@@ -356,6 +356,20 @@ static void inter(orc* o)                                                   /* s
 {
     int nc = o->nc, nv = o->nv, NP = nv + 1;
     if (o->c.order == 2) {
+        double ee1[6] = {0, 0, 0, 0, 0, 0};
+        if (o->c.limiter_type == 1) {                                        /* limiter.c:61-94 */
+            double mn[6], mx[6];
+            for (int kk = 0; kk < nv; kk++) mn[kk] = mx[kk] = o->P[kk == 4 ? 5 : kk];
+            for (int i = 1; i < nc; i++)
+                for (int kk = 0; kk < nv; kk++) {
+                    mn[kk] = fmin(mn[kk], o->P[(size_t)i * NP + (kk == 4 ? 5 : kk)]);
+                    mx[kk] = fmax(mx[kk], o->P[(size_t)i * NP + (kk == 4 ? 5 : kk)]);
+                }
+            for (int kk = 0; kk < nv; kk++) {
+                double a = (mx[kk] - mn[kk]) * o->c.limiter_k;
+                ee1[kk] = a * a;
+            }
+        }
         for (int i = 0; i < nc; i++) {
             double x0, y0, aux = o->c.limiter_k * sqrt(o->omega[i] / o->volMax);
             aux = aux * aux * aux;
@@ -372,7 +386,7 @@ static void inter(orc* o)                                                   /* s
                     int p0 = o->nodes[4 * i + j], p1 = o->nodes[4 * i + (j + 1) % o->npts[i]];
                     double xm = (o->xy[2 * p0] + o->xy[2 * p1]) * 0.5, ym = (o->xy[2 * p0 + 1] + o->xy[2 * p1 + 1]) * 0.5;
                     double d2 = (o->dPx[(size_t)kk * nc + i] * (xm - x0) + o->dPy[(size_t)kk * nc + i] * (ym - y0));
-                    double p = lim_v2(Pi, mn, mx, d2, o->Pref20[kk] * aux);
+                    double p = lim_v2(Pi, mn, mx, d2, o->c.limiter_type == 1 ? ee1[kk] : o->Pref20[kk] * aux);
                     phi = j == 0 ? p : fmin(phi, p);
                 }
                 o->phi[(size_t)kk * nc + i] = phi;
@@ -531,9 +545,12 @@ static void residual_of(orc* o, double* U)
 
 static void step_rk(orc* o)                                                 /* solver.c:788-840 */
 {
-    static const double a1[1] = {1.0}, a3[3] = {0.1481, 0.4, 1.0}, a4[4] = {0.0833, 0.2069, 0.4265, 1.0},
-                        a5[5] = {0.0533, 0.1263, 0.2375, 0.4414, 1.0};
-    const double* a = o->c.stages == 1 ? a1 : o->c.stages == 3 ? a3 : o->c.stages == 4 ? a4 : a5;
+    /* two stages {1/2, 1} (midpoint rule) is an extension restated here for the engine's 2-stage RK; the
+       reference implements 1, 3, 4 and 5 stages */
+    static const double a1[1] = {1.0}, a2[2] = {0.5, 1.0}, a3[3] = {0.1481, 0.4, 1.0},
+                        a4[4] = {0.0833, 0.2069, 0.4265, 1.0}, a5[5] = {0.0533, 0.1263, 0.2375, 0.4414, 1.0};
+    const double* a = o->c.stages == 1 ? a1 : o->c.stages == 2 ? a2 : o->c.stages == 3 ? a3
+                      : o->c.stages == 4 ? a4 : a5;
     for (int s = 0; s < o->c.stages; s++) {
         residual_of(o, s == 0 ? o->U : o->Uaux);
         rk_stage(o, a[s]);

@@ -1,0 +1,41 @@
+"""Limiter type 1 (limiterUpdate, limiter.c:61-94: epsilon from the global range of each variable) against
+the reference: one residual evaluation and its limiter bit for bit, and the state after 8 iterations."""
+import numpy as np
+import pytest
+
+import casekit
+
+pytestmark = pytest.mark.gpu
+
+# the cylinder with this limiter blows up within 10 iterations in the reference; with more than one RK
+# stage the engine's and the reference's blow-ups part ways (see the note in the engine's design notes),
+# so it runs the 1-stage scheme here
+CASES = [("caseWedge", {"timeScheme": "DPLUR", "Nlinear": "4", "CFL": "10.0"}),
+         ("caseWedge", {"timeScheme": "RK", "stages": "5", "CFL": "0.5"}),
+         ("caseCylinder", {"stages": "1"}),
+         ("caseBL_turb", {"restart": "0"})]
+
+
+@pytest.mark.parametrize("name,kv", CASES, ids=["%s_%s" % (c[0], c[1].get("timeScheme", "RK")) for c in CASES])
+def test_limiter_type1(native, name, kv):
+    import csu_b200
+    from oracle.refharness import Ref, available
+    if not available():
+        pytest.skip("reference build oracle/_ref missing")
+    wd = casekit.materialize(name, dict(kv, limiter="1", order="2"))
+    eng = csu_b200.Engine(csu_b200.Case.load(wd))
+    ref = Ref(wd)
+    R_ref = ref.calc_R()
+    R = eng.residual()
+    assert np.array_equal(R, R_ref), "%d residual entries differ" % np.count_nonzero(R != R_ref)
+    assert np.array_equal(eng.dump("PHI"), ref.phi())
+    eng.close()
+    eng = csu_b200.Engine(csu_b200.Case.load(wd))
+    ref = Ref(wd)
+    eng.iterate(8)
+    ref.iterate(8, 0)
+    U, U_ref = eng.get_state(), ref.get_U()
+    err = np.max(np.abs(U - U_ref) / np.abs(U_ref).max(axis=1, keepdims=True))
+    print("\n%s: state after 8 iterations %.2e" % (name, err))
+    assert err < 1e-12
+    eng.close()
