@@ -440,9 +440,8 @@ static int validate_config(const char* who, const csu_config* cfg, int* model_ou
                       "branch for SST and calls 4x4 DPLUR blocks with 6 variables); sstTrans not yet available", who);
         return CSU_ERR_UNSUPPORTED;
     }
-    if (model == 1 && (cfg->flux == CSU_FLUX_ROE || cfg->sa_cc)) {
-        csu_set_error("%s: SA with %s is not available (the reference has no Roe branch for SA)", who,
-                      cfg->sa_cc ? "saCC" : "Roe");
+    if (model == 1 && cfg->sa_cc) {
+        csu_set_error("%s: saCC is not available in this engine build", who);
         return CSU_ERR_UNSUPPORTED;
     }
     if (cfg->time_scheme == CSU_TS_LUSGS && model == 2) {

@@ -441,6 +441,12 @@ __device__ __forceinline__ void riemann(int scheme, const Gas& g, double eFix, d
     switch (scheme) {
     case 0:
         if constexpr (MODEL == 0) fluxRoe(g, eFix, L, Rr, f);
+        if constexpr (MODEL == 1) {
+            // extension: the reference's flux_sa has no Roe branch (flux.c:1325-1345); Roe for the mean flow,
+            // the SA working variable carried by the Roe mass flux from the upwind side
+            fluxRoe(g, eFix, L, Rr, f);
+            f[4] = f[0] * (f[0] > 0.0 ? L[4] : Rr[4]);
+        }
         break;
     case 1: fluxAUSM<MODEL>(g, L, Rr, f); break;
     case 2: fluxAUSMDV<MODEL>(g, L, Rr, f); break;

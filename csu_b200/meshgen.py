@@ -9,6 +9,7 @@ seeded and deterministic.
     bump(...)      channel with a 10 %-height circular bump, mixed triangles and quads
     cylinder(...)  cylinder (r = 0.5) in a 40-diameter box, O-grid
     airfoil(...)   NACA 0012 (closed trailing edge) C-mesh with wake cut, first cell y1
+    plate(...)     turbulent flat plate: tanh clustering at the leading edge, geometric wall spacing
 """
 import math
 import os
@@ -169,6 +170,48 @@ def cylinder(ncells=20000, mach=2.0, radius=0.5, box=40.0, tri_fraction=0.0, see
     kv.update({"BC:wall": "wall", "BC:farin": "inlet", "BC:farout": "outlet"})
     kv.update(_solver_kv(viscous=viscous, **solver))
     return _su2(pts, cells, markers), _input(kv)
+
+
+def plate(ni=545, nj=385, x0=-0.33, x1=2.0, height=1.0, y1=1e-6, growth=1.07, beta=3.0, mach=0.2, re=5e6,
+          temperature=300.0, viscous="sa", **solver):
+    """Flat plate: [x0, x1] x [0, height] m, no-slip adiabatic wall on x in [0, x1] and symmetry upstream.
+    ni x nj quads; x clustered at the leading edge with tanh stretching (factor `beta`) on both sides; y with
+    first spacing y1 growing geometrically by `growth` until the spacing that fills the height evenly is
+    reached. Re based on the plate length x1. Inlet left, outlet right, characteristic far field on top."""
+    n_up = max(2, int(round(ni * (-x0) / (x1 - x0))))
+    n_dn = ni - n_up
+    su = np.tanh(beta * np.linspace(0.0, 1.0, n_up + 1)) / np.tanh(beta)
+    sd = np.tanh(beta * np.linspace(0.0, 1.0, n_dn + 1)) / np.tanh(beta)
+    x = np.concatenate([x0 * su[::-1], x1 * sd[1:]])
+    ys = [0.0]
+    dy = y1
+    for k in range(nj):
+        rest = nj - k
+        even = (height - ys[-1]) / rest
+        if dy >= even:
+            ys.extend(list(ys[-1] + even * np.arange(1, rest + 1)))
+            break
+        ys.append(ys[-1] + dy)
+        dy *= growth
+    y = np.array(ys[:nj + 1])
+    y[-1] = height
+    X, Y = np.meshgrid(x, y)
+    pts, q, idx = _structured_quads(X, Y)
+    i_le = n_up
+    bottom = np.stack([idx[0, :-1], idx[0, 1:]], axis=1)
+    markers = {
+        "inlet": np.stack([idx[1:, 0], idx[:-1, 0]], axis=1),
+        "outlet": np.stack([idx[:-1, -1], idx[1:, -1]], axis=1),
+        "top": np.stack([idx[-1, 1:], idx[-1, :-1]], axis=1),
+        "sym": bottom[:i_le],
+        "plate": bottom[i_le:],
+    }
+    p = _pressure_for_re(re, mach, temperature, x1)
+    kv = _flow_kv(mach, p, temperature)
+    kv.update({"BC:inlet": "inlet", "BC:outlet": "outlet", "BC:top": "inlet", "BC:sym": "symmetry",
+               "BC:plate": "wall"})
+    kv.update(_solver_kv(viscous=viscous, **solver))
+    return _su2(pts, list(q), markers), _input(kv)
 
 
 def naca0012(x):
