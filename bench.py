@@ -125,9 +125,11 @@ def alg_bytes(case):
         "grad": nc * (W + 4 + 8 + 56 + G) + slots * (4 + 16 + 16) + nb * 28,
         # face index/normal/|dS|/two centre offsets + flux out; boundary face data + flux out; cell W and G in
         "flux": nf * (8 + 16 + 8 + 32 + 32) + nb * (4 + 4 + 16 + 8 + 32) + nc * (W + G),
-        # W, U, counts, omega; face flux per face; face geometry; per interior slot fslot + 16 FP64 block out;
-        # R, Omega/Lc, diagonal out
-        "impl": nc * (W + 32 + 8 + 8 + 32 + 8 + 8) + slots * 4 + (nf + nb) * 32 + nf * 32 + nb * 24 + nint * 128,
+        # W, counts, omega; face flux per face; face geometry; per slot fslot; R, Omega/Lc, diagonal out
+        "impl": nc * (W + 8 + 8 + 32 + 8 + 8) + slots * 4 + (nf + nb) * 32 + nf * 32 + nb * 24,
+        # U and W of every cell (as a neighbour), counts; face cells, normal, |dS|; per interior slot fslot +
+        # the 16 FP64 block out
+        "blocks": nc * (32 + W + 4) + nf * 32 + nint * (4 + 128),
         # x in, x out, counts, R, diagonal part, omega; per interior slot fslot + 16 FP64 block; face cells
         "sweep": nc * (32 + 32 + 4 + 32 + 8 + 8) + nint * (4 + 128) + nf * 8,
     }
@@ -252,10 +254,10 @@ def main():
 
     # per-kernel device times of a few iterations, for the roofline of the dominant kernel
     kt = eng.time_kernels(5)
-    names = ["prim", "grad", "flux", "rk", "impl", "sweep", "finalize", "resid"]
+    names = ["prim", "grad", "flux", "rk", "impl", "sweep", "finalize", "resid", "blocks"]
     per = {n: (kt["ms"][i] / kt["count"][i] if kt["count"][i] else 0.0) for i, n in enumerate(names)}
     share = {n: kt["ms"][i] for i, n in enumerate(names)}
-    dom = max(("grad", "flux", "impl", "sweep"), key=lambda n: share[n])
+    dom = max(("grad", "flux", "impl", "sweep", "blocks"), key=lambda n: share[n])
     ab = alg_bytes(case)
     peak, peak_kind = peaks()
     achieved = ab[dom] / (per[dom] * 1e-3) / 1e9

@@ -283,8 +283,8 @@ class Engine:
 
     def time_kernels(self, iters):
         """Device time per kernel kind over `iters` iterations (the state advances)."""
-        ms = (C.c_double * 8)()
-        cnt = (C.c_int * 8)()
+        ms = (C.c_double * 9)()
+        cnt = (C.c_int * 9)()
         _check(lib().csu_time_kernels(self._h, iters, ms, cnt))
         return {"ms": list(ms), "count": list(cnt)}
 

@@ -66,6 +66,10 @@ struct csu_ctx {
     long long graph_launches = 0;
     int have_debug = 0;
     cudaStream_t own_stream = nullptr;
+    // DPLUR blocks run on a side stream, forked from and joined back to the engine stream
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    int max_ni = 4;          // most interior faces of a cell (k_blocks covers slots [0, max_ni))
     // kernel timing (csu_time_kernels): an event after every launch, tagged with the kernel kind
     bool timing = false;
     std::vector<cudaEvent_t> ev;
@@ -74,7 +78,7 @@ struct csu_ctx {
 };
 
 // kinds of csu_time_kernels
-enum { KPRIM = 0, KGRAD, KFLUX, KRK, KIMPL, KSWEEP, KFIN, KRESID, KCOUNT };
+enum { KPRIM = 0, KGRAD, KFLUX, KRK, KIMPL, KSWEEP, KFIN, KRESID, KBLK, KCOUNT };
 
 static void tmark(csu_ctx* x, int kind)
 {
@@ -484,6 +488,13 @@ static int validate_config(const char* who, const csu_config* cfg, int* model_ou
 }
 
 // Allocates and fills the device side of x (x->L, x->prms and the pack offsets set by the caller).
+static int max_nint(const csu_layout& L)
+{
+    int m = 1;
+    for (int c = 0; c < L.nc; c++) m = std::max(m, L.nint[c]);
+    return m;
+}
+
 static int ctx_setup(csu_ctx* x)
 {
     int st;
@@ -501,9 +512,13 @@ static int ctx_setup(csu_ctx* x)
     plan(x, x->arena);
     e = cudaMemset(x->arena.base, 0, bytes);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&x->own_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&x->side, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&x->ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&x->ev_join, cudaEventDisableTiming);
     x->stream = x->own_stream;
     if (e != cudaSuccess) return cuda_fail(e, "context setup");
     x->gb_c = (x->L.nc + BLOCK - 1) / BLOCK;
+    if (x->L.nint) x->max_ni = max_nint(x->L); // packs set it from their solves
     x->gb_fi = (x->L.nf + BLOCK - 1) / BLOCK;
     x->gb_fb = (x->L.nb + BLOCK - 1) / BLOCK;
     if (!x->is_pack && (st = upload_mesh(x))) return st; // packs: pack_build fills the mesh rows
@@ -569,6 +584,9 @@ extern "C" void csu_destroy(csu_ctx* x)
     if (x->hist) cudaFree(x->hist);
     for (cudaEvent_t e : x->ev) cudaEventDestroy(e);
     if (x->own_stream) cudaStreamDestroy(x->own_stream);
+    if (x->side) cudaStreamDestroy(x->side);
+    if (x->ev_fork) cudaEventDestroy(x->ev_fork);
+    if (x->ev_join) cudaEventDestroy(x->ev_join);
     if (x->arena.base) cudaFree(x->arena.base);
     csu_layout_free(&x->L);
     delete x;
@@ -709,6 +727,24 @@ static void launch_prologue(csu_ctx* x)
     launch_finalize<MODEL>(x, 2);
 }
 
+// DPLUR blocks of this iteration on the side stream, forked from the engine stream at ev_fork (recorded by
+// the caller before the kernels they run beside, which are launched first so that their blocks are dispatched
+// first and k_blocks fills the SMs their last wave leaves idle); the first sweep joins. Timed runs keep them
+// on the engine stream, so each kernel kind's events bracket it alone.
+template <int MODEL>
+static void launch_blocks(csu_ctx* x)
+{
+    cudaStream_t s = x->stream;
+    if (!x->timing) {
+        cudaStreamWaitEvent(x->side, x->ev_fork, 0);
+        s = x->side;
+    }
+    k_blocks<MODEL><<<x->max_ni * x->gb_c, BLOCK, 0, s>>>(x->d_prm, x->mesh, x->st, x->gb_c);
+    x->launches++;
+    if (x->timing) tmark(x, KBLK);
+    else cudaEventRecord(x->ev_join, x->side);
+}
+
 // one iteration of the steady loop body (solver.c:1866-1906)
 template <int MODEL>
 static void launch_iteration(csu_ctx* x)
@@ -728,7 +764,7 @@ static void launch_iteration(csu_ctx* x)
     } else if (c.time_scheme == CSU_TS_LUSGS) {
         if (c.order == 2 || x->prm.visc) launch_grad<MODEL>(x, false);
         launch_flux<MODEL>(x, 1);
-        k_impl<MODEL, false><<<x->gb_c, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st);
+        k_impl<MODEL><<<x->gb_c, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st);
         x->launches++;
         tmark(x, KIMPL);
         const int K = x->L.ncolors;
@@ -752,11 +788,21 @@ static void launch_iteration(csu_ctx* x)
         tmark(x, KPRIM);
         launch_finalize<MODEL>(x, 1);
     } else {
-        if (c.order == 2 || x->prm.visc) launch_grad<MODEL>(x, false);
+        // the SA blocks need the face eddy viscosity of k_flux; the others only the iteration's start state
+        constexpr bool early = MODEL != 1;
+        const bool grad = c.order == 2 || x->prm.visc;
+        if (!x->timing) cudaEventRecord(x->ev_fork, x->stream);
+        if (grad) launch_grad<MODEL>(x, false);
+        if (early) launch_blocks<MODEL>(x);
         launch_flux<MODEL>(x, 1);
-        k_impl<MODEL, true><<<x->gb_c, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st);
+        if (!early) {
+            if (!x->timing) cudaEventRecord(x->ev_fork, x->stream);
+            launch_blocks<MODEL>(x);
+        }
+        k_impl<MODEL><<<x->gb_c, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st);
         x->launches++;
         tmark(x, KIMPL);
+        if (!x->timing) cudaStreamWaitEvent(x->stream, x->ev_join, 0);
         for (int m = 0; m < c.n_linear; m++) {
             if (m == c.n_linear - 1)
                 k_sweep<MODEL, true><<<x->gb_c, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st, m, x->xcur);
@@ -1579,6 +1625,8 @@ static int pack_build(const char* who, const csu_prep* const* solves, int n, csu
     x->ncs.resize(n);
     x->n2o.resize(n);
     memset(&x->L, 0, sizeof(x->L));
+    x->max_ni = 1;
+    for (int k = 0; k < n; k++) x->max_ni = std::max(x->max_ni, max_nint(solves[k]->L));
     int NC = 0, NF = 0, NB = 0, K = 0, walls = 0;
     std::vector<int> rank;
     for (int k = 0; k < n; k++) {

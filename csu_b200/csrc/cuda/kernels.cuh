@@ -776,10 +776,9 @@ __device__ __forceinline__ void aux_flux(const double* U, double pr, double nx, 
 }
 
 // ------------------------------------------------------------------------------------------------
-// k_impl: R, the implicit diagonal (implicitCalcD, implicit.c:19-181) and, with BLOCKS, the DPLUR
-// off-diagonal blocks of implicitUpdateA (implicit.c:689-813) for each interior face of the cell.
+// k_impl: R and the implicit diagonal (implicitCalcD, implicit.c:19-181) of each cell.
 // ------------------------------------------------------------------------------------------------
-template <int MODEL, bool BLOCKS>
+template <int MODEL>
 __global__ void __launch_bounds__(BLOCK) k_impl(const Prm* __restrict__ P, const __grid_constant__ Mesh m,
                                                 const __grid_constant__ State s)
 {
@@ -851,72 +850,96 @@ __global__ void __launch_bounds__(BLOCK) k_impl(const Prm* __restrict__ P, const
         s.dtl[c] = l;
         s.dpart[c] = D;
         lmin = l;
-        if (BLOCKS) {
-            const double h = 1.0e-6;
-            for (int j = 0; j < ni; j++) {
-                int sf = m.fslot[(size_t)j * nc + c];
-                int f = sf > 0 ? sf - 1 : -sf - 1;
-                int2 e = m.fe[f];
-                int nb = sf > 0 ? e.y : e.x;
-                double2 dSv = m.fn[f];
-                double dSx = sf > 0 ? dSv.x : -dSv.x, dSy = sf > 0 ? dSv.y : -dSv.y;
-                double dS = m.fds[f];
-                double nx = dSx / dS, ny = dSy / dS;
-                double Un[NV], Pn[NP];
-                loadU<MODEL>(s, nc, nb, Un);
-                loadP<MODEL>(s, nc, nb, Pn);
-                double F0[NV], F[NV], Uq[NV];
-                double rho = Un[0];
-                double uu = Un[1] / rho;
-                double vv = Un[2] / rho;
-                double E = Un[3] / rho;
-                aux_flux<NV>(Un, Pn[3], nx, ny, F0);
-                double ee0 = E - 0.5 * (uu * uu + vv * vv);
-                double A[NV * NV];
-#pragma unroll
-                for (int mm = 0; mm < NV; mm++) {
-#pragma unroll
-                    for (int nn = 0; nn < NV; nn++) Uq[nn] = mm == nn ? Un[nn] + h : Un[nn];
-                    double r2 = Uq[0];
-                    double u2 = Uq[1] / r2;
-                    double v2 = Uq[2] / r2;
-                    double E2 = Uq[3] / r2;
-                    double ee1 = E2 - 0.5 * (u2 * u2 + v2 * v2);
-                    double T = e2Taprox(p.gas, ee0, Pn[4], ee1);
-                    double pr = p.gas.R * r2 * T;
-                    aux_flux<NV>(Uq, pr, nx, ny, F);
-#pragma unroll
-                    for (int nn = 0; nn < NV; nn++) A[nn * NV + mm] = 0.5 * (F[nn] - F0[nn]) * dS / h;
-                }
-                double cc = T2c(p.gas, Pn[4]);
-                double ra = p.w_imp * (fabs(nx * Pn[1] + ny * Pn[2]) + cc) * dS;
-                if constexpr (MODEL == 1) {
-                    // implicitUpdateA_sa (implicit.c:920-928): always viscous, with the face eddy viscosity
-                    double r = (P[0] + Pn[0]) * 0.5;
-                    double T = (P[4] + Pn[4]) * 0.5;
-                    double mi = sutherland(T);
-                    ra += fmax(4 / (3 * r), T2gamma(p.gas, T) / r) * (mi / p.pr + s.MIT[f] / p.pr_t) * dS / m.fL[f];
-                } else if (p.laminar) {
-                    double r = (P[0] + Pn[0]) * 0.5;
-                    double T = (P[4] + Pn[4]) * 0.5;
-                    ra += visc_radius(p.gas, p.pr, r, T) * dS / m.fL[f];
-                }
-#pragma unroll
-                for (int nn = 0; nn < NV; nn++) A[nn * NV + nn] -= 0.5 * ra;
-                const size_t base = (size_t)j * NV * NV * nc + c;
-                if (p.blk32) {
-#pragma unroll
-                    for (int q = 0; q < NV * NV; q++) s.blocks32[base + (size_t)q * nc] = (float)A[q];
-                } else {
-#pragma unroll
-                    for (int q = 0; q < NV * NV; q++) s.blocks[base + (size_t)q * nc] = A[q];
-                }
-            }
-        }
     }
     double v = warp_min(lmin);
     if ((threadIdx.x & 31) == 0 && !(v > bitsd(0x7fefffffffffffffULL))) atomicMin(&sc->dtmin_bits, dbits(v));
     partial_norms<MODEL>(s, valid, R);
+}
+
+// ------------------------------------------------------------------------------------------------
+// k_blocks: the DPLUR off-diagonal blocks of implicitUpdateA (implicit.c:689-813; implicitUpdateA_sa
+// 860-935), one thread per interior face slot j of a cell: the finite-difference Jacobian (h = 1e-6) of the
+// neighbour's face flux, minus half the face's spectral radius on the diagonal. A block needs only the
+// state at the start of the iteration (and, for SA, the face eddy viscosity of k_flux), so the engine runs
+// this kernel beside the gradient and flux kernels. Blocks [j gb, (j + 1) gb) of the grid hold slot j of
+// the cells of cell blocks [0, gb).
+// ------------------------------------------------------------------------------------------------
+template <int MODEL>
+__global__ void __launch_bounds__(BLOCK, 3) k_blocks(const Prm* __restrict__ P, const __grid_constant__ Mesh m,
+                                                  const __grid_constant__ State s, int gb)
+{
+    constexpr int NV = Model<MODEL>::NV, NP = Model<MODEL>::NP;
+    const int j = blockIdx.x / gb, cb = blockIdx.x - j * gb;
+    const int sid = s.bsolve ? s.bsolve[cb] : 0;
+    const Prm& p = P[sid];
+    const Scalars* const sc = s.sc + sid;
+    if (halted(sc)) return;
+    const int c = cb * BLOCK + threadIdx.x;
+    if (!cell_in(p, c)) return;
+    const int nc = m.nc;
+    if (j >= m.nint[c]) return;
+    const int sf = m.fslot[(size_t)j * nc + c];
+    const int f = sf > 0 ? sf - 1 : -sf - 1;
+    const int2 e = m.fe[f];
+    const int nb = sf > 0 ? e.y : e.x;
+    const double2 dSv = m.fn[f];
+    const double dSx = sf > 0 ? dSv.x : -dSv.x, dSy = sf > 0 ? dSv.y : -dSv.y;
+    const double dS = m.fds[f];
+    const double nx = dSx / dS, ny = dSy / dS;
+    const double h = 1.0e-6;
+    double Un[NV], Pn[NP];
+    loadU<MODEL>(s, nc, nb, Un);
+    loadP<MODEL>(s, nc, nb, Pn);
+    double F0[NV], F[NV], Uq[NV];
+    double rho = Un[0];
+    double uu = Un[1] / rho;
+    double vv = Un[2] / rho;
+    double E = Un[3] / rho;
+    aux_flux<NV>(Un, Pn[3], nx, ny, F0);
+    double ee0 = E - 0.5 * (uu * uu + vv * vv);
+    double A[NV * NV];
+#pragma unroll
+    for (int mm = 0; mm < NV; mm++) {
+#pragma unroll
+        for (int nn = 0; nn < NV; nn++) Uq[nn] = mm == nn ? Un[nn] + h : Un[nn];
+        double r2 = Uq[0];
+        double u2 = Uq[1] / r2;
+        double v2 = Uq[2] / r2;
+        double E2 = Uq[3] / r2;
+        double ee1 = E2 - 0.5 * (u2 * u2 + v2 * v2);
+        double T = e2Taprox(p.gas, ee0, Pn[4], ee1);
+        double pr = p.gas.R * r2 * T;
+        aux_flux<NV>(Uq, pr, nx, ny, F);
+#pragma unroll
+        for (int nn = 0; nn < NV; nn++) A[nn * NV + mm] = 0.5 * (F[nn] - F0[nn]) * dS / h;
+    }
+    double cc = T2c(p.gas, Pn[4]);
+    double ra = p.w_imp * (fabs(nx * Pn[1] + ny * Pn[2]) + cc) * dS;
+    if constexpr (MODEL == 1) {
+        // implicitUpdateA_sa (implicit.c:920-928): always viscous, with the face eddy viscosity
+        double Pc[NP];
+        loadP<MODEL>(s, nc, c, Pc);
+        double r = (Pc[0] + Pn[0]) * 0.5;
+        double T = (Pc[4] + Pn[4]) * 0.5;
+        double mi = sutherland(T);
+        ra += fmax(4 / (3 * r), T2gamma(p.gas, T) / r) * (mi / p.pr + s.MIT[f] / p.pr_t) * dS / m.fL[f];
+    } else if (p.laminar) {
+        double Pc[NP];
+        loadP<MODEL>(s, nc, c, Pc);
+        double r = (Pc[0] + Pn[0]) * 0.5;
+        double T = (Pc[4] + Pn[4]) * 0.5;
+        ra += visc_radius(p.gas, p.pr, r, T) * dS / m.fL[f];
+    }
+#pragma unroll
+    for (int nn = 0; nn < NV; nn++) A[nn * NV + nn] -= 0.5 * ra;
+    const size_t base = (size_t)j * NV * NV * nc + c;
+    if (p.blk32) {
+#pragma unroll
+        for (int q = 0; q < NV * NV; q++) s.blocks32[base + (size_t)q * nc] = (float)A[q];
+    } else {
+#pragma unroll
+        for (int q = 0; q < NV * NV; q++) s.blocks[base + (size_t)q * nc] = A[q];
+    }
 }
 
 // ------------------------------------------------------------------------------------------------

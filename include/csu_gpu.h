@@ -210,11 +210,12 @@ int csu_set_stream(csu_ctx* ctx, void* stream);
 #define CSU_K_GRAD 1     /* least-squares gradient + limiter (solverUpdateGrad, inter)    */
 #define CSU_K_FLUX 2     /* interior and boundary face fluxes (inter, boundary)           */
 #define CSU_K_RK 3       /* residual gather + RK stage (solverRK)                         */
-#define CSU_K_IMPL 4     /* residual gather + implicit diagonal + DPLUR blocks            */
+#define CSU_K_IMPL 4     /* residual gather + implicit diagonal                           */
 #define CSU_K_SWEEP 5    /* one DPLUR Jacobi sweep                                        */
 #define CSU_K_FINALIZE 6 /* norms, force coefficients, step size                          */
 #define CSU_K_RESID 7    /* residual gather only                                          */
-#define CSU_K_COUNT 8
+#define CSU_K_BLOCKS 8   /* DPLUR off-diagonal blocks (finite-difference face Jacobians)  */
+#define CSU_K_COUNT 9
 /* Runs `iters` iterations with a CUDA event after every kernel and returns, per kind, the summed device
  * time in ms and the launch count (the iterations advance the state like csu_iterate). */
 int csu_time_kernels(csu_ctx* ctx, int iters, double* ms, int* count);
