@@ -141,6 +141,7 @@ static void plan(csu_ctx* x, Arena& a)
     m.ex = carve<double>(a, c4);
     m.ey = carve<double>(a, c4);
     m.fslot = carve<int>(a, c4);
+    m.fnb = carve<int>(a, c4);
     m.omega = carve<double>(a, nc);
     m.sxh = carve<double>(a, nc);
     m.syh = carve<double>(a, nc);
@@ -274,6 +275,7 @@ static int upload_mesh(csu_ctx* x)
     CK(up(m.ex, L.ex, sizeof(double) * c4));
     CK(up(m.ey, L.ey, sizeof(double) * c4));
     CK(up(m.fslot, L.fslot, sizeof(int) * c4));
+    CK(up(m.fnb, L.fnb, sizeof(int) * c4));
     CK(up(m.omega, L.omega, sizeof(double) * nc));
     CK(up(m.sxh, L.sxh, sizeof(double) * nc));
     CK(up(m.syh, L.syh, sizeof(double) * nc));
@@ -1426,7 +1428,7 @@ static std::vector<SegArr> seg_arrays(csu_ctx* x)
         {P(m.nei), 4, SEG_CELL4}, {P(m.wx), 8, SEG_CELL4}, {P(m.wy), 8, SEG_CELL4},
         {P(m.ldx), 8, SEG_CELL4}, {P(m.ldy), 8, SEG_CELL4}, {P(m.lm), 8, SEG_CELL4},
         {P(m.les), 4, SEG_CELL4}, {P(m.lrv), 8, SEG_CELL}, {P(m.lq), 16, SEG_CELL4},
-        {P(m.ex), 8, SEG_CELL4}, {P(m.ey), 8, SEG_CELL4}, {P(m.fslot), 4, SEG_CELL4},
+        {P(m.ex), 8, SEG_CELL4}, {P(m.ey), 8, SEG_CELL4}, {P(m.fslot), 4, SEG_CELL4}, {P(m.fnb), 4, SEG_CELL4},
         {P(m.omega), 8, SEG_CELL}, {P(m.sxh), 8, SEG_CELL}, {P(m.syh), 8, SEG_CELL},
         {P(m.dslat), 8, SEG_CELL}, {P(m.color), 4, SEG_CELL},
         {P(m.fe), 8, SEG_FACE}, {P(m.fn), 16, SEG_FACE}, {P(m.fds), 8, SEG_FACE}, {P(m.r0), 16, SEG_FACE},
@@ -1469,7 +1471,7 @@ static std::vector<const void*> seg_host(const csu_layout& L, std::vector<std::v
     int* rank = (int*)keep.back().data();
     local_wall_ranks(L, rank);
     std::vector<const void*> v = {
-        L.npts, L.nint, L.nslot, L.nei, L.wx, L.wy, L.ldx, L.ldy, L.lm, L.les, L.lrv, L.lq, L.ex, L.ey, L.fslot,
+        L.npts, L.nint, L.nslot, L.nei, L.wx, L.wy, L.ldx, L.ldy, L.lm, L.les, L.lrv, L.lq, L.ex, L.ey, L.fslot, L.fnb,
         L.omega, L.sxh, L.syh, L.dslat, L.color,
         fe, pairs(L.fdsx, L.fdsy, nf), L.fds, pairs(L.r0x, L.r0y, nf), pairs(L.r1x, L.r1y, nf),
         pairs(L.fdx, L.fdy, nf), L.fdist,
@@ -1488,8 +1490,10 @@ __global__ void k_seg_fix(Mesh m, int* wall_rank, SegGeo S, SegGeo D)
         int c = D.c0 + t;
         int* nei = const_cast<int*>(m.nei);
         int* fs = const_cast<int*>(m.fslot);
+        int* fnb = const_cast<int*>(m.fnb);
         for (int j = 0; j < 4; j++) {
             size_t o = (size_t)j * D.NC + c;
+            if (fnb[o] >= 0) fnb[o] += dc;
             int v = nei[o];
             nei[o] = v < S.NC ? v + dc : v - S.NC - S.b0 + D.NC + D.b0;
             int f = fs[o];

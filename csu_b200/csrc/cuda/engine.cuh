@@ -89,6 +89,7 @@ struct Mesh {
     const unsigned long long* lrv;  // reciprocal of det's significand
     const double2* lq;              // [4][nc] a, b, c and 1/det as exact (h, l) double-doubles
     const int* fslot;
+    const int* fnb;                 // [4][nc] neighbour across interior face slot j, else -1
     const double* omega;
     const double* sxh;
     const double* syh;
@@ -417,6 +418,33 @@ __device__ __forceinline__ double warp_max(double v)
 {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Block-wide minimum / maximum, valid in thread 0; every thread of the block calls them. They let a kernel
+// take one atomic per block on a solve's scalar instead of one per warp: atomics on one address serialise
+// at the L2, and one per warp of a 160k-cell grid costs microseconds.
+__device__ __forceinline__ double block_min(double v)
+{
+    __shared__ double sh[BLOCK / 32];
+    v = warp_min(v);
+    __syncthreads(); // an earlier call may still read sh
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int w = 1; w < BLOCK / 32; w++) v = fmin(v, sh[w]);
+    return v;
+}
+
+__device__ __forceinline__ double block_max(double v)
+{
+    __shared__ double sh[BLOCK / 32];
+    v = warp_max(v);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int w = 1; w < BLOCK / 32; w++) v = fmax(v, sh[w]);
     return v;
 }
 

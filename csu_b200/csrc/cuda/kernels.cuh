@@ -70,8 +70,8 @@ __global__ void __launch_bounds__(BLOCK) k_prim(const Prm* __restrict__ P, const
         storeP<MODEL>(s, m.nc, c, P);
     }
     if (with_dt) {
-        double v = warp_min(lmin);
-        if ((threadIdx.x & 31) == 0 && !(v > bitsd(0x7fefffffffffffffULL))) atomicMin(&sc->dtmin_bits, dbits(v));
+        double v = block_min(lmin);
+        if (threadIdx.x == 0 && !(v > bitsd(0x7fefffffffffffffULL))) atomicMin(&sc->dtmin_bits, dbits(v));
     }
 }
 
@@ -756,8 +756,8 @@ __global__ void __launch_bounds__(BLOCK) k_rk(const Prm* __restrict__ P, const _
         storeP<MODEL>(s, m.nc, c, P);
     }
     if (LAST) {
-        double v = warp_min(lmin);
-        if ((threadIdx.x & 31) == 0 && !(v > bitsd(0x7fefffffffffffffULL))) atomicMin(&sc->dtmin_bits, dbits(v));
+        double v = block_min(lmin);
+        if (threadIdx.x == 0 && !(v > bitsd(0x7fefffffffffffffULL))) atomicMin(&sc->dtmin_bits, dbits(v));
         partial_norms<MODEL>(s, valid, R);
     }
 }
@@ -851,8 +851,8 @@ __global__ void __launch_bounds__(BLOCK) k_impl(const Prm* __restrict__ P, const
         s.dpart[c] = D;
         lmin = l;
     }
-    double v = warp_min(lmin);
-    if ((threadIdx.x & 31) == 0 && !(v > bitsd(0x7fefffffffffffffULL))) atomicMin(&sc->dtmin_bits, dbits(v));
+    double v = block_min(lmin);
+    if (threadIdx.x == 0 && !(v > bitsd(0x7fefffffffffffffULL))) atomicMin(&sc->dtmin_bits, dbits(v));
     partial_norms<MODEL>(s, valid, R);
 }
 
@@ -984,30 +984,41 @@ __global__ void __launch_bounds__(BLOCK) k_sweep(const Prm* __restrict__ P, cons
             double y[NV];
 #pragma unroll
             for (int k = 0; k < NV; k++) y[k] = D * xo[k];
+            // Slots 0-2 are gathered unconditionally (a slot without a face reads the cell itself and a zero
+            // block, both in bounds, and is not summed), so their index and neighbour loads issue together
+            // instead of one dependent chain per face; slot 3 only exists in quadrilaterals.
             const int ni = m.nint[c];
-            for (int j = 0; j < ni; j++) {
-                int sf = m.fslot[(size_t)j * nc + c];
-                int f = sf > 0 ? sf - 1 : -sf - 1;
-                int2 e = m.fe[f];
-                int nb = sf > 0 ? e.y : e.x;
+            int nbj[4];
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                int q = m.fnb[(size_t)j * nc + c];
+                nbj[j] = q >= 0 ? q : c;
+            }
+            nbj[3] = ni > 3 ? m.fnb[(size_t)3 * nc + c] : c;
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                if (j == 3 && ni <= 3) break;
+                const int nb = nbj[j];
                 double xb[NV];
                 double4 t = xo4[nb];
                 xb[0] = t.x; xb[1] = t.y; xb[2] = t.z; xb[3] = t.w;
 #pragma unroll
                 for (int k = 4; k < NV; k++) xb[k] = xox[(size_t)(k - 4) * nc + nb];
                 const size_t base = (size_t)j * NV * NV * nc + c;
+                const bool use = j < ni;
+                double A[NV * NV];
                 if (p.blk32) {
-                    const float* A = s.blocks32 + base;
 #pragma unroll
-                    for (int kk = 0; kk < NV; kk++)
-#pragma unroll
-                        for (int nn = 0; nn < NV; nn++) y[kk] += (double)A[(size_t)(kk * NV + nn) * nc] * xb[nn];
+                    for (int q = 0; q < NV * NV; q++) A[q] = (double)s.blocks32[base + (size_t)q * nc];
                 } else {
-                    const double* A = s.blocks + base;
+#pragma unroll
+                    for (int q = 0; q < NV * NV; q++) A[q] = s.blocks[base + (size_t)q * nc];
+                }
+                if (use) {
 #pragma unroll
                     for (int kk = 0; kk < NV; kk++)
 #pragma unroll
-                        for (int nn = 0; nn < NV; nn++) y[kk] += A[(size_t)(kk * NV + nn) * nc] * xb[nn];
+                        for (int nn = 0; nn < NV; nn++) y[kk] += A[kk * NV + nn] * xb[nn];
                 }
             }
             double R[NV];
@@ -1036,8 +1047,8 @@ __global__ void __launch_bounds__(BLOCK) k_sweep(const Prm* __restrict__ P, cons
         }
     }
     if (!conv) {
-        double v = warp_max(dmax);
-        if ((threadIdx.x & 31) == 0) atomicMax(&sc->sweep_max[sweep], dbits(v));
+        double v = block_max(dmax);
+        if (threadIdx.x == 0) atomicMax(&sc->sweep_max[sweep], dbits(v));
     }
 }
 
@@ -1217,7 +1228,10 @@ __global__ void __launch_bounds__(BLOCK) k_finalize(const Prm* __restrict__ P, c
     const int npart = p.nblk, nwall = p.nwall;
     const double* part = s.part + (size_t)p.blk0 * NV;
     const double* bcoef = s.bcoef + (size_t)p.wall0 * 4;
-    if (mode != 2 && mode != 3 && halted(sc)) return;
+    // Everything the block reads is requested before the halted test, so the loads overlap: a chain of
+    // dependent round trips to the L2 would be most of a one-block kernel's time. Thread 0 keeps a copy of
+    // the solve's scalars and writes back only what changes.
+    const bool stop = mode != 2 && mode != 3 && halted(sc);
     double v[NV + 4];
 #pragma unroll
     for (int k = 0; k < NV + 4; k++) v[k] = 0.0;
@@ -1232,13 +1246,18 @@ __global__ void __launch_bounds__(BLOCK) k_finalize(const Prm* __restrict__ P, c
 #pragma unroll
             for (int k = 0; k < 4; k++) v[NV + k] += bcoef[(size_t)i * 4 + k];
     }
+    Scalars S;
+    if (threadIdx.x == 0) S = *sc;
+    if (stop) return;
     block_sum<NV + 4>(v, sh);
     if (threadIdx.x != 0) return;
     if (mode != 2) {
         bool bad = false;
+        double res[NV];
         for (int k = 0; k < NV; k++) {
-            sc->res[k] = sqrt(v[k] / p.nc);
-            if (!isfinite(sc->res[k])) bad = true;
+            res[k] = sqrt(v[k] / p.nc);
+            sc->res[k] = res[k];
+            if (!isfinite(res[k])) bad = true;
         }
         // Cx_v -= fx/q per wall face (solver.c:1376-1380): the negated sum
         double cxp = v[NV] / p.sref, cyp = v[NV + 1] / p.sref;
@@ -1249,39 +1268,43 @@ __global__ void __launch_bounds__(BLOCK) k_finalize(const Prm* __restrict__ P, c
         }
         sc->coef[0] = cxp; sc->coef[1] = cxv; sc->coef[2] = cyp; sc->coef[3] = cyv;
         if (mode == 3) return;
-        if (sc->hist && sc->hist_row < sc->hist_cap) {
-            double* row = sc->hist + (size_t)sc->hist_row * (NV + 4);
-            for (int k = 0; k < NV; k++) row[k] = sc->res[k];
+        if (S.hist && S.hist_row < S.hist_cap) {
+            double* row = S.hist + (size_t)S.hist_row * (NV + 4);
+            for (int k = 0; k < NV; k++) row[k] = res[k];
             row[NV] = cxp; row[NV + 1] = cxv; row[NV + 2] = cyp; row[NV + 3] = cyv;
         }
-        sc->hist_row++;
-        if (!sc->have_res0) {
-            for (int k = 0; k < NV; k++) sc->res0[k] = sc->res[k];
+        sc->hist_row = S.hist_row + 1;
+        double r00 = S.res0[0];
+        if (!S.have_res0) {
+            for (int k = 0; k < NV; k++) sc->res0[k] = res[k];
             sc->have_res0 = 1;
+            r00 = res[0];
         }
-        sc->steps++;
-        if (sc->iter == p.dt_local_n) sc->dt_local = 0;
-        sc->iter++;
+        sc->steps = S.steps + 1;
+        if (S.iter == p.dt_local_n) sc->dt_local = 0;
+        S.iter++;
+        sc->iter = S.iter;
         if (bad) sc->status = 4; // CSU_ERR_NONFINITE
         if (p.tube) {
-            sc->t += sc->dt * p.stages / 2.0;
-            if (sc->stop_after) sc->done = 1;
+            S.t += S.dt * p.stages / 2.0;
+            sc->t = S.t;
+            if (S.stop_after) sc->done = 1;
         }
-        if (p.conv_tol > 0 && sc->res[0] <= p.conv_tol * sc->res0[0]) sc->done = 1;
-        else if (p.iter_cap > 0 && sc->iter >= p.iter_cap) sc->done = 2;
+        if (p.conv_tol > 0 && res[0] <= p.conv_tol * r00) sc->done = 1;
+        else if (p.iter_cap > 0 && S.iter >= p.iter_cap) sc->done = 2;
         for (int k = 0; k < MAX_SWEEPS; k++) sc->sweep_max[k] = 0ULL;
     }
-    if (mode == 2 && !sc->fresh) {
+    if (mode == 2 && !S.fresh) {
         sc->dtmin_bits = 0x7ff0000000000000ULL;
         return;
     }
     if (mode == 2) sc->fresh = 0;
     if (mode == 0 || mode == 2) {
         // solverCalcDt (solver.c:925-950) for the next iteration, from the minimum gathered above
-        double dt = bitsd(sc->dtmin_bits);
-        dt *= cfl_at(p, sc->iter);
-        if (p.tube && sc->t + dt > p.tmax) {
-            dt = (p.tmax - sc->t);
+        double dt = bitsd(S.dtmin_bits);
+        dt *= cfl_at(p, S.iter);
+        if (p.tube && S.t + dt > p.tmax) {
+            dt = (p.tmax - S.t);
             sc->stop_after = 1;
         }
         sc->dt = dt;

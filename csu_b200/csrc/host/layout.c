@@ -112,7 +112,7 @@ void csu_layout_free(csu_layout* L)
 {
     void* ptrs[] = {L->cell_new2old, L->cell_old2new, L->face_new2old, L->face_old2new, L->bface_new2old,
                     L->bface_old2new, L->npts, L->nint, L->nslot, L->nei, L->wx, L->wy, L->ex, L->ey,
-                    L->fslot, L->omega, L->sxh, L->syh, L->xc, L->yc, L->wall_d, L->dslat, L->fe0, L->fe1,
+                    L->fslot, L->fnb, L->omega, L->sxh, L->syh, L->xc, L->yc, L->wall_d, L->dslat, L->fe0, L->fe1,
                     L->fdsx, L->fdsy, L->fds, L->r0x, L->r0y, L->r1x, L->r1y, L->fdist, L->bown, L->bflag,
                     L->bold, L->bdsx, L->bdsy, L->bds, L->bmx, L->bmy, L->ldx, L->ldy, L->lm, L->les, L->lrv, L->lq,
                     L->fdx, L->fdy, L->bdx, L->bdy, L->bL, L->bunx, L->buny, L->bds2, L->color,
@@ -134,7 +134,7 @@ int csu_layout_build(const csu_mesh_desc* m, int axi, csu_layout* L)
     ALLOC(L->face_new2old, nf); ALLOC(L->face_old2new, nf);
     ALLOC(L->bface_new2old, nb); ALLOC(L->bface_old2new, nb);
     ALLOC(L->npts, nc); ALLOC(L->nint, nc); ALLOC(L->nslot, nc); ALLOC(L->nei, c4);
-    ALLOC(L->wx, c4); ALLOC(L->wy, c4); ALLOC(L->ex, c4); ALLOC(L->ey, c4); ALLOC(L->fslot, c4);
+    ALLOC(L->wx, c4); ALLOC(L->wy, c4); ALLOC(L->ex, c4); ALLOC(L->ey, c4); ALLOC(L->fslot, c4); ALLOC(L->fnb, c4);
     ALLOC(L->ldx, c4); ALLOC(L->ldy, c4); ALLOC(L->lm, c4); ALLOC(L->les, c4); ALLOC(L->lrv, nc); ALLOC(L->lq, 2 * c4);
     ALLOC(L->omega, nc); ALLOC(L->sxh, nc); ALLOC(L->syh, nc); ALLOC(L->xc, nc); ALLOC(L->yc, nc);
     ALLOC(L->dslat, nc);
@@ -374,6 +374,14 @@ int csu_layout_build(const csu_mesh_desc* m, int axi, csu_layout* L)
         L->fslot[(size_t)ns * nc + c] = nf + bn + 1;
         L->nslot[c] = ns + 1;
     }
+    /* neighbour across each interior face slot (the sweeps gather through it in one step) */
+    for (size_t q = 0; q < c4; q++) L->fnb[q] = -1;
+    for (int c = 0; c < nc; c++)
+        for (int j = 0; j < L->nint[c]; j++) {
+            int sf = L->fslot[(size_t)j * nc + c];
+            int f = (sf > 0 ? sf : -sf) - 1;
+            L->fnb[(size_t)j * nc + c] = sf > 0 ? L->fe1[f] : L->fe0[f];
+        }
     /* greedy colouring in the renumbered (Hilbert) order: the multicolour Gauss-Seidel of LU-SGS */
     L->color = malloc(sizeof(int) * (nc > 0 ? nc : 1));
     L->ncolors = 0;

@@ -39,6 +39,7 @@ typedef struct csu_layout {
     double* ex;    /* [4][nc] edge midpoint minus centroid, edges in node order (limiter, inter)        */
     double* ey;
     int* fslot;    /* [4][nc] +-(flux index + 1): interior faces (ELEMENT.f order) then boundary faces  */
+    int* fnb;      /* [4][nc] the neighbour cell across interior face slot j (j < nint), else -1          */
     double* omega;
     double* sxh;   /* 0.5 * sum |dSx| over the cell edges (solverLocalTimeStep, solver.c:904-914)      */
     double* syh;
