@@ -733,6 +733,7 @@ static void launch_prologue(csu_ctx* x)
 // the caller before the kernels they run beside, which are launched first so that their blocks are dispatched
 // first and k_blocks fills the SMs their last wave leaves idle); the first sweep joins. Timed runs keep them
 // on the engine stream, so each kernel kind's events bracket it alone.
+// The implicit diagonal and step (k_impl without R) go on the same side stream.
 template <int MODEL>
 static void launch_blocks(csu_ctx* x)
 {
@@ -744,7 +745,21 @@ static void launch_blocks(csu_ctx* x)
     k_blocks<MODEL><<<x->max_ni * x->gb_c, BLOCK, 0, s>>>(x->d_prm, x->mesh, x->st, x->gb_c);
     x->launches++;
     if (x->timing) tmark(x, KBLK);
+    k_impl<MODEL, false><<<x->gb_c, BLOCK, 0, s>>>(x->d_prm, x->mesh, x->st);
+    x->launches++;
+    if (x->timing) tmark(x, KIMPL);
     else cudaEventRecord(x->ev_join, x->side);
+}
+
+template <int MODEL>
+static void launch_sweep(csu_ctx* x, int m, int n)
+{
+    auto* k = m == 0 ? (m == n - 1 ? k_sweep<MODEL, true, true> : k_sweep<MODEL, false, true>)
+                     : (m == n - 1 ? k_sweep<MODEL, true, false> : k_sweep<MODEL, false, false>);
+    k<<<x->gb_c, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st, m, x->xcur);
+    x->launches++;
+    tmark(x, KSWEEP);
+    x->xcur ^= 1;
 }
 
 // one iteration of the steady loop body (solver.c:1866-1906)
@@ -766,7 +781,7 @@ static void launch_iteration(csu_ctx* x)
     } else if (c.time_scheme == CSU_TS_LUSGS) {
         if (c.order == 2 || x->prm.visc) launch_grad<MODEL>(x, false);
         launch_flux<MODEL>(x, 1);
-        k_impl<MODEL><<<x->gb_c, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st);
+        k_impl<MODEL, true><<<x->gb_c, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st);
         x->launches++;
         tmark(x, KIMPL);
         const int K = x->L.ncolors;
@@ -790,7 +805,8 @@ static void launch_iteration(csu_ctx* x)
         tmark(x, KPRIM);
         launch_finalize<MODEL>(x, 1);
     } else {
-        // the SA blocks need the face eddy viscosity of k_flux; the others only the iteration's start state
+        // the SA blocks and diagonal need the face eddy viscosity of k_flux; the others only the iteration's
+        // start state
         constexpr bool early = MODEL != 1;
         const bool grad = c.order == 2 || x->prm.visc;
         if (!x->timing) cudaEventRecord(x->ev_fork, x->stream);
@@ -801,18 +817,9 @@ static void launch_iteration(csu_ctx* x)
             if (!x->timing) cudaEventRecord(x->ev_fork, x->stream);
             launch_blocks<MODEL>(x);
         }
-        k_impl<MODEL><<<x->gb_c, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st);
-        x->launches++;
-        tmark(x, KIMPL);
         if (!x->timing) cudaStreamWaitEvent(x->stream, x->ev_join, 0);
-        for (int m = 0; m < c.n_linear; m++) {
-            if (m == c.n_linear - 1)
-                k_sweep<MODEL, true><<<x->gb_c, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st, m, x->xcur);
-            else k_sweep<MODEL, false><<<x->gb_c, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st, m, x->xcur);
-            x->launches++;
-            tmark(x, KSWEEP);
-            x->xcur ^= 1;
-        }
+        // the first sweep gathers R (and its norms) from the face fluxes
+        for (int m = 0; m < c.n_linear; m++) launch_sweep<MODEL>(x, m, c.n_linear);
         launch_finalize<MODEL>(x, 1);
     }
 }

@@ -776,9 +776,11 @@ __device__ __forceinline__ void aux_flux(const double* U, double pr, double nx, 
 }
 
 // ------------------------------------------------------------------------------------------------
-// k_impl: R and the implicit diagonal (implicitCalcD, implicit.c:19-181) of each cell.
+// k_impl: R (WITH_R) and the implicit diagonal (implicitCalcD, implicit.c:19-181) of each cell. The
+// diagonal, the local steps and their minimum need only the iteration's start state, so DPLUR computes them
+// beside the gradient and flux kernels and gathers R in its first sweep.
 // ------------------------------------------------------------------------------------------------
-template <int MODEL>
+template <int MODEL, bool WITH_R>
 __global__ void __launch_bounds__(BLOCK) k_impl(const Prm* __restrict__ P, const __grid_constant__ Mesh m,
                                                 const __grid_constant__ State s)
 {
@@ -795,8 +797,10 @@ __global__ void __launch_bounds__(BLOCK) k_impl(const Prm* __restrict__ P, const
         const int nc = m.nc;
         double P[NP];
         loadP<MODEL>(s, nc, c, P);
-        gather_residual<MODEL>(p, m, s, c, P, R);
-        storeR<MODEL>(s, nc, c, R);
+        if (WITH_R) {
+            gather_residual<MODEL>(p, m, s, c, P, R);
+            storeR<MODEL>(s, nc, c, R);
+        }
         const int ni = m.nint[c], ns = m.nslot[c];
         double Lc = 0, Lv = 0;
         for (int j = 0; j < ni; j++) {
@@ -853,7 +857,7 @@ __global__ void __launch_bounds__(BLOCK) k_impl(const Prm* __restrict__ P, const
     }
     double v = block_min(lmin);
     if (threadIdx.x == 0 && !(v > bitsd(0x7fefffffffffffffULL))) atomicMin(&sc->dtmin_bits, dbits(v));
-    partial_norms<MODEL>(s, valid, R);
+    if (WITH_R) partial_norms<MODEL>(s, valid, R);
 }
 
 // ------------------------------------------------------------------------------------------------
@@ -947,9 +951,11 @@ __global__ void __launch_bounds__(BLOCK, 3) k_blocks(const Prm* __restrict__ P, 
 //   x_new = w (-R - (D x + sum_j A_j x_j)) / D + x,  w = 2/3,  D += Omega/dt with dt = CFL min(Omega/Lc).
 // The early exit of the reference (max |dx_0| < 1e-14 after a sweep) is taken on the device: a sweep that
 // finds the previous one converged copies x forward. LAST adds the increment to the state
-// (solverUpdateUImplicit, solver.c:1945-1955) and computes the next iteration's primitives.
+// (solverUpdateUImplicit, solver.c:1945-1955) and computes the next iteration's primitives. FIRST gathers
+// the cell's residual R from the face fluxes (as k_impl does), stores it for the later sweeps and writes
+// the block's partial norms.
 // ------------------------------------------------------------------------------------------------
-template <int MODEL, bool LAST>
+template <int MODEL, bool LAST, bool FIRST>
 __global__ void __launch_bounds__(BLOCK) k_sweep(const Prm* __restrict__ P, const __grid_constant__ Mesh m,
                                                  const __grid_constant__ State s, int sweep, int cur)
 {
@@ -960,9 +966,11 @@ __global__ void __launch_bounds__(BLOCK) k_sweep(const Prm* __restrict__ P, cons
     if (halted(sc)) return;
     int c = blockIdx.x * BLOCK + threadIdx.x;
     const int nc = m.nc;
-    bool conv = sweep > 0 && bitsd(sc->sweep_max[sweep - 1]) < 1e-14;
+    bool conv = !FIRST && sweep > 0 && bitsd(sc->sweep_max[sweep - 1]) < 1e-14;
     double dmax = 0.0;
-    if (cell_in(p, c)) {
+    const bool valid = cell_in(p, c);
+    double R[NV];
+    if (valid) {
         const double4* xo4 = s.X4[cur];
         const double* xox = s.Xx[cur];
         double4* xn4 = s.X4[cur ^ 1];
@@ -973,6 +981,17 @@ __global__ void __launch_bounds__(BLOCK) k_sweep(const Prm* __restrict__ P, cons
             xo[0] = t.x; xo[1] = t.y; xo[2] = t.z; xo[3] = t.w;
 #pragma unroll
             for (int k = 4; k < NV; k++) xo[k] = xox[(size_t)(k - 4) * nc + c];
+        }
+        if constexpr (FIRST) {
+            double Pc[NP];
+            loadP<MODEL>(s, nc, c, Pc);
+            gather_residual<MODEL>(p, m, s, c, Pc, R);
+            storeR<MODEL>(s, nc, c, R);
+        } else {
+            double4 t = s.R4[c];
+            R[0] = t.x; R[1] = t.y; R[2] = t.z; R[3] = t.w;
+#pragma unroll
+            for (int k = 4; k < NV; k++) R[k] = s.Rx[(size_t)(k - 4) * nc + c];
         }
         if (conv) {
 #pragma unroll
@@ -1021,13 +1040,6 @@ __global__ void __launch_bounds__(BLOCK) k_sweep(const Prm* __restrict__ P, cons
                         for (int nn = 0; nn < NV; nn++) y[kk] += A[kk * NV + nn] * xb[nn];
                 }
             }
-            double R[NV];
-            {
-                double4 t = s.R4[c];
-                R[0] = t.x; R[1] = t.y; R[2] = t.z; R[3] = t.w;
-#pragma unroll
-                for (int k = 4; k < NV; k++) R[k] = s.Rx[(size_t)(k - 4) * nc + c];
-            }
             const double w = 2. / 3.;
 #pragma unroll
             for (int k = 0; k < NV; k++) xn[k] = w * (-R[k] - y[k]) / D + xo[k];
@@ -1050,6 +1062,7 @@ __global__ void __launch_bounds__(BLOCK) k_sweep(const Prm* __restrict__ P, cons
         double v = block_max(dmax);
         if (threadIdx.x == 0) atomicMax(&sc->sweep_max[sweep], dbits(v));
     }
+    if (FIRST) partial_norms<MODEL>(s, valid, R);
 }
 
 // implicitCalcDeltaFlux (implicit.c:194-231) and implicitCalcDeltaFlux_sa (495-552): F(U + d) - F(U) on the
