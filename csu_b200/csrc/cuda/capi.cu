@@ -59,7 +59,7 @@ struct csu_ctx {
     int xcur = 0;
     long long launches = 0;
     int hist_cap = 0;
-    int gb_c = 0, gb_fi = 0, gb_fb = 0;
+    int gb_c = 0;
     const double* rk = nullptr;
     cudaGraphExec_t graph = nullptr;
     int graph_iters = 0;
@@ -521,8 +521,6 @@ static int ctx_setup(csu_ctx* x)
     if (e != cudaSuccess) return cuda_fail(e, "context setup");
     x->gb_c = (x->L.nc + BLOCK - 1) / BLOCK;
     if (x->L.nint) x->max_ni = max_nint(x->L); // packs set it from their solves
-    x->gb_fi = (x->L.nf + BLOCK - 1) / BLOCK;
-    x->gb_fb = (x->L.nb + BLOCK - 1) / BLOCK;
     if (!x->is_pack && (st = upload_mesh(x))) return st; // packs: pack_build fills the mesh rows
     x->prm = x->prms[0];
     if ((st = upload_prm(x)) || (st = reset_scalars(x, 0))) return st;
@@ -702,11 +700,16 @@ static void launch_grad(csu_ctx* x, bool dbg)
     tmark(x, KGRAD);
 }
 
+// faces in blocks of FLUX_BLOCK threads (more resident blocks per SM, finer waves)
+#ifndef FLUX_BLOCK
+#define FLUX_BLOCK 64
+#endif
 template <int MODEL>
 static void launch_flux(csu_ctx* x, int coef)
 {
-    k_flux<MODEL><<<x->gb_fi + x->gb_fb, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st, x->gb_fi, x->d_wall_rank,
-                                                                 coef);
+    constexpr int FB = FLUX_BLOCK;
+    const int gi = (x->L.nf + FB - 1) / FB, gb = (x->L.nb + FB - 1) / FB;
+    k_flux<MODEL, FB><<<gi + gb, FB, 0, x->stream>>>(x->d_prm, x->mesh, x->st, gi, x->d_wall_rank, coef);
     x->launches++;
     tmark(x, KFLUX);
 }
@@ -751,12 +754,21 @@ static void launch_blocks(csu_ctx* x)
     else cudaEventRecord(x->ev_join, x->side);
 }
 
+// Sweeps after the first run in blocks of SWEEP_BLOCK threads (more resident blocks per SM, finer waves).
+#ifndef SWEEP_BLOCK
+#define SWEEP_BLOCK 128
+#endif
 template <int MODEL>
 static void launch_sweep(csu_ctx* x, int m, int n)
 {
-    auto* k = m == 0 ? (m == n - 1 ? k_sweep<MODEL, true, true> : k_sweep<MODEL, false, true>)
-                     : (m == n - 1 ? k_sweep<MODEL, true, false> : k_sweep<MODEL, false, false>);
-    k<<<x->gb_c, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st, m, x->xcur);
+    constexpr int SB = SWEEP_BLOCK;
+    if (m == 0) {
+        auto* k = m == n - 1 ? k_sweep<MODEL, true, true, BLOCK> : k_sweep<MODEL, false, true, BLOCK>;
+        k<<<x->gb_c, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st, m, x->xcur);
+    } else {
+        auto* k = m == n - 1 ? k_sweep<MODEL, true, false, SB> : k_sweep<MODEL, false, false, SB>;
+        k<<<x->gb_c * (BLOCK / SB), SB, 0, x->stream>>>(x->d_prm, x->mesh, x->st, m, x->xcur);
+    }
     x->launches++;
     tmark(x, KSWEEP);
     x->xcur ^= 1;

@@ -436,15 +436,16 @@ __device__ __forceinline__ double block_min(double v)
     return v;
 }
 
+template <int NT = BLOCK>
 __device__ __forceinline__ double block_max(double v)
 {
-    __shared__ double sh[BLOCK / 32];
+    __shared__ double sh[NT / 32];
     v = warp_max(v);
     __syncthreads();
     if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
     __syncthreads();
     if (threadIdx.x == 0)
-        for (int w = 1; w < BLOCK / 32; w++) v = fmax(v, sh[w]);
+        for (int w = 1; w < NT / 32; w++) v = fmax(v, sh[w]);
     return v;
 }
 

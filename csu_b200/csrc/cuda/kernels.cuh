@@ -418,15 +418,15 @@ __global__ void __launch_bounds__(BLOCK, 2) k_grad(const Prm* __restrict__ P, co
 // k_flux: interior faces (blocks [0, nbi)) and boundary faces (blocks [nbi, ...)).
 // coef: also record the wall pressure-coefficient terms of solverCalcCoeff3 (solver.c:1360-1385).
 // ------------------------------------------------------------------------------------------------
-template <int MODEL>
-__global__ void __launch_bounds__(BLOCK) k_flux(const Prm* __restrict__ P, const __grid_constant__ Mesh m,
-                                                const __grid_constant__ State s, int nbi, const int* wall_rank,
-                                                int coef)
+template <int MODEL, int FB>
+__global__ void __launch_bounds__(FB) k_flux(const Prm* __restrict__ P, const __grid_constant__ Mesh m,
+                                             const __grid_constant__ State s, int nbi, const int* wall_rank,
+                                             int coef)
 {
     constexpr int NV = Model<MODEL>::NV, NP = Model<MODEL>::NP;
     const int nc = m.nc;
     if ((int)blockIdx.x < nbi) {
-        int f = blockIdx.x * BLOCK + threadIdx.x;
+        int f = blockIdx.x * FB + threadIdx.x;
         if (f >= m.nf) return;
         int2 e = m.fe[f];
         const int sid = cell_solve(s, e.x);
@@ -510,7 +510,7 @@ __global__ void __launch_bounds__(BLOCK) k_flux(const Prm* __restrict__ P, const
 #pragma unroll
         for (int kk = 4; kk < NV; kk++) s.Fx[(size_t)(kk - 4) * (m.nf + m.nb) + f] = fl[kk] * dS;
     } else {
-        int b = (blockIdx.x - nbi) * BLOCK + threadIdx.x;
+        int b = (blockIdx.x - nbi) * FB + threadIdx.x;
         if (b >= m.nb) return;
         int c = m.bown[b];
         const int sid = cell_solve(s, c);
@@ -955,16 +955,18 @@ __global__ void __launch_bounds__(BLOCK, 3) k_blocks(const Prm* __restrict__ P, 
 // the cell's residual R from the face fluxes (as k_impl does), stores it for the later sweeps and writes
 // the block's partial norms.
 // ------------------------------------------------------------------------------------------------
-template <int MODEL, bool LAST, bool FIRST>
-__global__ void __launch_bounds__(BLOCK) k_sweep(const Prm* __restrict__ P, const __grid_constant__ Mesh m,
-                                                 const __grid_constant__ State s, int sweep, int cur)
+template <int MODEL, bool LAST, bool FIRST, int SB>
+__global__ void __launch_bounds__(SB) k_sweep(const Prm* __restrict__ P, const __grid_constant__ Mesh m,
+                                              const __grid_constant__ State s, int sweep, int cur)
 {
     constexpr int NV = Model<MODEL>::NV, NP = Model<MODEL>::NP;
-    const int sid = block_solve(s);
+    static_assert(BLOCK % SB == 0 && (!FIRST || SB == BLOCK), "sweep blocks tile the cell blocks");
+    // SB-thread blocks: BLOCK / SB of them cover one cell block of the solve map
+    const int sid = s.bsolve ? s.bsolve[blockIdx.x / (BLOCK / SB)] : 0;
     const Prm& p = P[sid];
     Scalars* const sc = s.sc + sid;
     if (halted(sc)) return;
-    int c = blockIdx.x * BLOCK + threadIdx.x;
+    int c = blockIdx.x * SB + threadIdx.x;
     const int nc = m.nc;
     bool conv = !FIRST && sweep > 0 && bitsd(sc->sweep_max[sweep - 1]) < 1e-14;
     double dmax = 0.0;
@@ -1059,7 +1061,7 @@ __global__ void __launch_bounds__(BLOCK) k_sweep(const Prm* __restrict__ P, cons
         }
     }
     if (!conv) {
-        double v = block_max(dmax);
+        double v = block_max<SB>(dmax);
         if (threadIdx.x == 0) atomicMax(&sc->sweep_max[sweep], dbits(v));
     }
     if (FIRST) partial_norms<MODEL>(s, valid, R);
