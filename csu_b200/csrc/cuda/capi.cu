@@ -206,6 +206,8 @@ static void plan(csu_ctx* x, Arena& a)
     x->d_prm = carve<Prm>(a, x->nsolve);
     s.dbg_ghost = carve<double>(a, (size_t)(nb > 0 ? nb : 1) * (nv + 1));
     s.lsq_x87 = carve<unsigned long long>(a, 1);
+    s.gfix = carve<int2>(a, (size_t)nc * (nv + 1)); // at most one entry per cell and variable (and T)
+    s.gfix_n = carve<unsigned>(a, 2);
 }
 
 static int upload_mesh(csu_ctx* x)
@@ -682,7 +684,12 @@ static void launch_grad_lsq(csu_ctx* x)
     switch (x->prm.lsq_exact) {
     case 0: k_grad<MODEL, DBG, 0><<<x->gb_c, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st); break;
     case 1: k_grad<MODEL, DBG, 1><<<x->gb_c, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st); break;
-    default: k_grad<MODEL, DBG, 2><<<x->gb_c, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st); break;
+    default:
+        // the rare components left undecided by the FP64 paths are finished by k_grad_fix
+        k_grad<MODEL, DBG, 2><<<x->gb_c, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st);
+        k_grad_fix<MODEL><<<2 * 148, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st);
+        x->launches++;
+        break;
     }
 }
 

@@ -80,7 +80,7 @@ __global__ void __launch_bounds__(BLOCK) k_prim(const Prm* __restrict__ P, const
 // DBG also records ghost primitives (boundaryCalcPrimitive) in reference order.
 // LSQ selects the least-squares arithmetic (Prm::lsq_exact): 0 precomputed FP64 weights, 1 the integer x87
 // model (ext80.cuh) for every component, 2 the FP64 x87 emulation and certified double-double solve of
-// lsqdd.cuh, with the integer model only for the rare components those cannot decide (lsq_slot_x87).
+// lsqdd.cuh, with the integer model only for the rare components those cannot decide (k_grad_fix).
 // ------------------------------------------------------------------------------------------------
 
 // x87 constants a, b, c, det of cell c (solver.c:1063-1073, evaluated on the host in long double)
@@ -105,9 +105,11 @@ __device__ __forceinline__ double limiter_eps2(const Prm& p, const Scalars* sc, 
 }
 
 // One gradient component pair of cell c for primitive vi (T: 4) with the integer x87 model, gathering the
-// neighbours again. Out of line: only the rare components the FP64 path cannot decide come here.
+// neighbours again; also the cell's value of the primitive and its range over the cell and the neighbours
+// (the limiter's inputs). Only the rare components the FP64 path cannot decide come here (k_grad_fix).
 template <int MODEL>
-__device__ __forceinline__ double2 lsq_slot_x87(const Prm& p, const Mesh& m, const State& s, int c, int vi)
+__device__ __forceinline__ double2 lsq_slot_x87(const Prm& p, const Mesh& m, const State& s, int c, int vi,
+                                                double* u0p, double* qminp, double* qmaxp)
 {
     constexpr int NP = Model<MODEL>::NP;
     const int nc = m.nc;
@@ -117,6 +119,9 @@ __device__ __forceinline__ double2 lsq_slot_x87(const Prm& p, const Mesh& m, con
 #pragma unroll
     for (int k = 0; k < NP; k++)
         if (k == vi) u0 = P0[k];
+    *u0p = u0;
+    *qminp = u0;
+    *qmaxp = u0;
     X80 XA = x80_zero(0), XB = x80_zero(0);
     const int np = m.npts[c];
     const double dw = m.wall_d ? m.wall_d[c] : 0.0;
@@ -135,6 +140,8 @@ __device__ __forceinline__ double2 lsq_slot_x87(const Prm& p, const Mesh& m, con
         for (int k = 0; k < NP; k++)
             if (k == vi) un = Pn[k];
         double du = un - u0;
+        *qmaxp = fmax(*qmaxp, un);
+        *qminp = fmin(*qminp, un);
         XA = x80_add(XA, x80_from_double(m.ldx[(size_t)j * nc + c] * du));
         XB = x80_add(XB, x80_from_double(m.ldy[(size_t)j * nc + c] * du));
     }
@@ -192,7 +199,7 @@ __global__ void __launch_bounds__(BLOCK) k_minmax(const Prm* __restrict__ P, con
 }
 
 template <int MODEL, bool DBG, int LSQ>
-__global__ void __launch_bounds__(BLOCK, 2) k_grad(const Prm* __restrict__ P, const __grid_constant__ Mesh m,
+__global__ void __launch_bounds__(BLOCK, 3) k_grad(const Prm* __restrict__ P, const __grid_constant__ Mesh m,
                                                 const __grid_constant__ State s)
 {
     constexpr int NV = Model<MODEL>::NV, NP = Model<MODEL>::NP;
@@ -339,7 +346,10 @@ __global__ void __launch_bounds__(BLOCK, 2) k_grad(const Prm* __restrict__ P, co
                     if (!lsq_certified(ka, kb, R, TY, TX, &gty)) need |= 2u << (2 * NV);
                 }
                 if (!sum_ok) need = visc ? (4u << (2 * NV)) - 1u : (1u << (2 * NV)) - 1u;
-                // one out-of-loop copy of the exact-numerator solve, then of the integer x87 model
+                // one out-of-loop copy of the exact-numerator solve; what that cannot decide (about one
+                // component in a thousand) is left to k_grad_fix and the integer x87 model, whose registers
+                // and code would otherwise slow every cell of this kernel
+                unsigned xneed = 0;
 #pragma unroll 1
                 while (need) {
                     const int b = __ffs(need) - 1;
@@ -356,10 +366,7 @@ __global__ void __launch_bounds__(BLOCK, 2) k_grad(const Prm* __restrict__ P, co
                     double g = 0.0;
                     bool ok = sum_ok && (comp ? lsq_exact_numerator(ka, kb, R, Y, X, &g)
                                               : lsq_exact_numerator(kc, kb, R, X, Y, &g));
-                    if (!ok) {
-                        double2 gg = lsq_slot_x87<MODEL>(p, m, s, c, kk < NV ? slot2p(kk) : 4);
-                        g = comp ? gg.y : gg.x;
-                    }
+                    if (!ok) xneed |= 1u << b;
                     if (kk == NV) {
                         if (comp) gty = g;
                         else gtx = g;
@@ -371,6 +378,12 @@ __global__ void __launch_bounds__(BLOCK, 2) k_grad(const Prm* __restrict__ P, co
                             else gx[q] = g;
                         }
                     }
+                }
+                // one k_grad_fix entry per (cell, variable) with undecided components
+#pragma unroll 1
+                for (int q = 0; q <= NV; q++) {
+                    const unsigned mk = (xneed >> (2 * q)) & 3u;
+                    if (mk) s.gfix[atomicAdd(s.gfix_n, 1u)] = make_int2(c, q | (int)(mk << 8));
                 }
             }
         }
@@ -410,6 +423,64 @@ __global__ void __launch_bounds__(BLOCK, 2) k_grad(const Prm* __restrict__ P, co
             s.Gxx[(size_t)(kk - 4) * nc + c] = gx[kk];
             s.Gxy[(size_t)(kk - 4) * nc + c] = gy[kk];
             s.PHx[(size_t)(kk - 4) * nc + c] = phi[kk];
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// k_grad_fix: the gradient components neither k_grad's certified solve nor its exact x87 numerator could
+// decide, entry (cell, variable kk (NV: temperature), mask of x / y): both components of the variable with
+// the integer x87 model (lsq_slot_x87), the undecided ones taken from it, then the variable's limiter
+// (limiterCalc) from the final gradient, as k_grad computes it. Grid-stride over the entries; the last block
+// to finish empties the list for the next gradient launch.
+// ------------------------------------------------------------------------------------------------
+template <int MODEL>
+__global__ void __launch_bounds__(BLOCK) k_grad_fix(const Prm* __restrict__ P, const __grid_constant__ Mesh m,
+                                                    const __grid_constant__ State s)
+{
+    constexpr int NV = Model<MODEL>::NV;
+    const unsigned n = *s.gfix_n;
+    const int nc = m.nc;
+    for (unsigned e = blockIdx.x * BLOCK + threadIdx.x; e < n; e += gridDim.x * BLOCK) {
+        const int2 w = s.gfix[e];
+        const int c = w.x, kk = w.y & 0xff, mask = w.y >> 8;
+        const int sid = cell_solve(s, c);
+        const Prm& p = P[sid];
+        const Scalars* sc = s.sc + sid;
+        double u0, qmin, qmax;
+        const double2 gg = lsq_slot_x87<MODEL>(p, m, s, c, kk < NV ? slot2p(kk) : 4, &u0, &qmin, &qmax);
+        // the components k_grad decided are already in place
+        double* gxp = kk == NV ? s.GTx + c : kk < 4 ? reinterpret_cast<double*>(s.G4x + c) + kk
+                                                      : s.Gxx + (size_t)(kk - 4) * nc + c;
+        double* gyp = kk == NV ? s.GTy + c : kk < 4 ? reinterpret_cast<double*>(s.G4y + c) + kk
+                                                      : s.Gxy + (size_t)(kk - 4) * nc + c;
+        const double gx = (mask & 1) ? gg.x : *gxp, gy = (mask & 2) ? gg.y : *gyp;
+        *gxp = gx;
+        *gyp = gy;
+        if (kk < NV && p.order == 2) {
+            double aux = p.lim_k * sqrt(m.omega[c] / p.vol_max);
+            aux = aux * aux * aux;
+            const double ee = limiter_eps2(p, sc, kk, aux);
+            const int np = m.npts[c];
+            double phi = 1.0;
+#pragma unroll 1
+            for (int j = 0; j < np; j++) {
+                double exj = m.ex[(size_t)j * nc + c], eyj = m.ey[(size_t)j * nc + c];
+                double d2 = (gx * exj + gy * eyj);
+                double phi0 = p.lim_func == 1 ? limiterBJ(u0, qmin, qmax, d2) : limiterV2(u0, qmin, qmax, d2, ee);
+                phi = j == 0 ? phi0 : fmin(phi, phi0);
+            }
+            if (kk < 4) reinterpret_cast<double*>(s.PH4 + c)[kk] = phi;
+            else s.PHx[(size_t)(kk - 4) * nc + c] = phi;
+        }
+    }
+    // every block read the count above before it counts itself done
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(s.gfix_n + 1, 1u) == gridDim.x - 1) {
+            s.gfix_n[0] = 0;
+            s.gfix_n[1] = 0;
         }
     }
 }

@@ -20,10 +20,11 @@
 // If the interval [q - E, q + E] around the double-double value q contains no rounding boundary of
 // double precision (a midpoint between two consecutive doubles), the x87 result rounds to the same
 // double as q, namely RN(q): the component is certified and returned. Otherwise (about one component in
-// a hundred: strong cancellation in the numerator, or q close to a midpoint) lsq_exact_numerator
-// computes the numerator exactly as x87 would and certifies only the division; what that cannot decide
-// (about one in a thousand) the caller recomputes with ext80.cuh.
-// Either way the result is the reference's bit pattern.
+// a hundred on solver meshes: strong cancellation in the numerator, or q close to a midpoint)
+// lsq_exact_numerator computes the numerator exactly as x87 would, then the x87 division's rounding to 64
+// bits from the double-double quotient and its bound, and the store to double exactly; what that cannot
+// decide (a quotient within 2^-100 of a boundary of the 64-bit grid: none in millions of random
+// components) the caller recomputes with ext80.cuh. Either way the result is the reference's bit pattern.
 #pragma once
 #include <math.h>
 #include <string.h>
@@ -261,8 +262,12 @@ X80_HD bool lsq_certified(DD k1, DD k2, DD R, DD X, DD Y, double* out)
 }
 
 // The same when lsq_certified cannot decide: the x87 numerator RN64(RN64(k1 X) - RN64(k2 Y)) computed
-// exactly (x87_mul, x87_add), so only the division's rounding is left to the bound. A zero numerator is
-// +0 in x87 (k1 > 0 and the sums are never -0), and so is the quotient.
+// exactly (x87_mul, x87_add), then the x87 division itself: RN64(N / det) decided on the 64-bit grid from
+// the double-double quotient N R (relative error <= 2^-103 (R) + 7 2^-106 (dd_mul) < 2^-102, bounded here by
+// 2^-100 |q|), and its store to double, RN53 of that 64-bit value, done exactly by the hardware addition in
+// x87_round's result (s = RN(h + q) of an exact sum). Undecidable only when the quotient lies within
+// 2^-100 of a midpoint of the 64-bit grid. A zero numerator is +0 in x87 (k1 > 0 and the sums are never
+// -0), and so is the quotient.
 X80_HD bool lsq_exact_numerator(DD k1, DD k2, DD R, DD X, DD Y, double* out)
 {
     bool ok = true;
@@ -277,9 +282,11 @@ X80_HD bool lsq_exact_numerator(DD k1, DD k2, DD R, DD X, DD Y, double* out)
         return true;
     }
     DD q = dd_mul(N, R);
-    double aq = fabs(q.h);
-    double E = 0x1p-64 * aq * (1.0 + 0x1p-20) + 0x1p-95 * aq;
-    return dd_round_certified(q, E, out);
+    DD r = {q.l, 0.0};
+    DD q64 = x87_round(q.h, r, 0x1p-100 * fabs(q.h), ok);
+    if (!ok) return false;
+    *out = q64.h;
+    return true;
 }
 
 } // namespace csu
