@@ -125,13 +125,17 @@ def alg_bytes(case):
         "grad": nc * (W + 4 + 8 + 56 + G) + slots * (4 + 16 + 16) + nb * 28,
         # face index/normal/|dS|/two centre offsets + flux out; boundary face data + flux out; cell W and G in
         "flux": nf * (8 + 16 + 8 + 32 + 32) + nb * (4 + 4 + 16 + 8 + 32) + nc * (W + G),
-        # W, counts, omega; face flux per face; face geometry; per slot fslot; R, Omega/Lc, diagonal out
-        "impl": nc * (W + 8 + 8 + 32 + 8 + 8) + slots * 4 + (nf + nb) * 32 + nf * 32 + nb * 24,
+        # DPLUR diagonal (k_impl without R): W, counts, omega; per slot fslot; face cells, normal, |dS|;
+        # boundary normal, |dS|; Omega/Lc and diagonal out
+        "impl": nc * (W + 8 + 8 + 8 + 8) + slots * 4 + nf * 32 + nb * 24,
         # U and W of every cell (as a neighbour), counts; face cells, normal, |dS|; per interior slot fslot +
         # the 16 FP64 block out
         "blocks": nc * (32 + W + 4) + nf * 32 + nint * (4 + 128),
-        # x in, x out, counts, R, diagonal part, omega; per interior slot fslot + 16 FP64 block; face cells
-        "sweep": nc * (32 + 32 + 4 + 32 + 8 + 8) + nint * (4 + 128) + nf * 8,
+        # mean of the four sweeps of an iteration: x in, x out, counts, R, diagonal part, omega; per interior
+        # slot its neighbour + 16 FP64 block; the first sweep also reads W, the face fluxes and the slots
+        # (R gather), the last reads and writes U and writes W
+        "sweep": nc * (32 + 32 + 4 + 32 + 8 + 8) + nint * (4 + 128)
+                 + (nc * W + (nf + nb) * 32 + slots * 4 + nc * (32 + 32 + W)) // 4,
     }
 
 
