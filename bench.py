@@ -283,7 +283,7 @@ def main():
     for i in range(e2e_steps):
         eng.set_state(host)
         eng.iterate(1, it0=i)
-        host[:] = eng.get_state()
+        eng.get_state(out=host)
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
     e2e = nc * e2e_steps * world / e2e_s

@@ -241,10 +241,16 @@ class Engine:
         U = np.ascontiguousarray(U, dtype=np.float64).reshape(self.nvar, self.n_cells)
         _check(lib().csu_set_state(self._h, _ptr(U)))
 
-    def get_state(self):
-        U = np.zeros((self.nvar, self.n_cells))
-        _check(lib().csu_get_state(self._h, _ptr(U)))
-        return U
+    def get_state(self, out=None):
+        """The conserved state [var][cell] in reference order. `out`: a C-contiguous float64 array of that
+        shape to fill (e.g. pinned host memory, which the device then writes by DMA) instead of a new one."""
+        if out is None:
+            out = np.empty((self.nvar, self.n_cells))
+        elif (out.dtype != np.float64 or not out.flags.c_contiguous or out.size != self.nvar * self.n_cells):
+            raise ValueError("get_state: out must be a C-contiguous float64 array of %d x %d"
+                             % (self.nvar, self.n_cells))
+        _check(lib().csu_get_state(self._h, _ptr(out)))
+        return out
 
     def residual(self):
         R = np.zeros((self.nvar, self.n_cells))

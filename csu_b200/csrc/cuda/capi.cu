@@ -70,6 +70,9 @@ struct csu_ctx {
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int max_ni = 4;          // most interior faces of a cell (k_blocks covers slots [0, max_ni))
+    // one-solve contexts: the renumbering on the device and a staging buffer for the state in reference order
+    int* d_n2o = nullptr;
+    double* d_stage = nullptr;
     // kernel timing (csu_time_kernels): an event after every launch, tagged with the kernel kind
     bool timing = false;
     std::vector<cudaEvent_t> ev;
@@ -208,6 +211,10 @@ static void plan(csu_ctx* x, Arena& a)
     s.lsq_x87 = carve<unsigned long long>(a, 1);
     s.gfix = carve<int2>(a, (size_t)nc * (nv + 1)); // at most one entry per cell and variable (and T)
     s.gfix_n = carve<unsigned>(a, 2);
+    if (!x->is_pack) {
+        x->d_n2o = carve<int>(a, nc);
+        x->d_stage = carve<double>(a, (size_t)nv * nc);
+    }
 }
 
 static int upload_mesh(csu_ctx* x)
@@ -278,6 +285,7 @@ static int upload_mesh(csu_ctx* x)
     CK(up(m.ey, L.ey, sizeof(double) * c4));
     CK(up(m.fslot, L.fslot, sizeof(int) * c4));
     CK(up(m.fnb, L.fnb, sizeof(int) * c4));
+    CK(up(x->d_n2o, L.cell_new2old, sizeof(int) * nc));
     CK(up(m.omega, L.omega, sizeof(double) * nc));
     CK(up(m.sxh, L.sxh, sizeof(double) * nc));
     CK(up(m.syh, L.syh, sizeof(double) * nc));
@@ -595,8 +603,52 @@ extern "C" void csu_destroy(csu_ctx* x)
 }
 
 // State of solve k in its reference order ([var][cell], nvar x its cell count), to or from the device.
+// The state of a one-solve context between reference order ([var][cell], in the staging buffer) and the
+// renumbered device layout (U4 + SoA scalars); k_state_in also marks the state as set from outside.
+__global__ void k_state_in(State s, const double* stage, const int* n2o, int nc, int nv)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c == 0) s.sc[0].fresh = 1;
+    if (c >= nc) return;
+    const int q = n2o[c];
+    s.U4[c] = make_double4(stage[q], stage[(size_t)nc + q], stage[(size_t)2 * nc + q], stage[(size_t)3 * nc + q]);
+    for (int r = 4; r < nv; r++) s.Ux[(size_t)(r - 4) * nc + c] = stage[(size_t)r * nc + q];
+}
+
+__global__ void k_state_out(State s, double* stage, const int* n2o, int nc, int nv)
+{
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nc) return;
+    const int q = n2o[c];
+    const double4 u = s.U4[c];
+    stage[q] = u.x;
+    stage[(size_t)nc + q] = u.y;
+    stage[(size_t)2 * nc + q] = u.z;
+    stage[(size_t)3 * nc + q] = u.w;
+    for (int r = 4; r < nv; r++) stage[(size_t)r * nc + q] = s.Ux[(size_t)(r - 4) * nc + c];
+}
+
 static int solve_state_io(csu_ctx* x, int k, double* U, bool put)
 {
+    if (!x->is_pack) {
+        // one copy of the caller's array (a DMA when it is pinned) and the renumbering on the device
+        const int nc = x->L.nc, nv = x->nv;
+        const size_t bytes = sizeof(double) * (size_t)nv * nc;
+        const int g = (nc + BLOCK - 1) / BLOCK;
+        if (put) {
+            CK(cudaMemcpyAsync(x->d_stage, U, bytes, cudaMemcpyHostToDevice, x->stream));
+            k_state_in<<<g, BLOCK, 0, x->stream>>>(x->st, x->d_stage, x->d_n2o, nc, nv);
+            CK(cudaGetLastError());
+            CK(cudaStreamSynchronize(x->stream)); // the caller may reuse U on return
+            x->prepared = 0;
+            return CSU_OK;
+        }
+        k_state_out<<<g, BLOCK, 0, x->stream>>>(x->st, x->d_stage, x->d_n2o, nc, nv);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(U, x->d_stage, bytes, cudaMemcpyDeviceToHost, x->stream));
+        CK(cudaStreamSynchronize(x->stream));
+        return CSU_OK;
+    }
     const int nck = x->ncs[k], o = x->cell0[k], NC = x->L.nc, nv = x->nv;
     // a pack keeps each solve's renumbering (its concatenated layout has none); a one-solve context its own
     const int* n2o = x->is_pack ? x->n2o[k].data() : x->L.cell_new2old;
@@ -687,7 +739,7 @@ static void launch_grad_lsq(csu_ctx* x)
     default:
         // the rare components left undecided by the FP64 paths are finished by k_grad_fix
         k_grad<MODEL, DBG, 2><<<x->gb_c, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st);
-        k_grad_fix<MODEL><<<2 * 148, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st);
+        k_grad_fix<MODEL><<<1, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st);
         x->launches++;
         break;
     }
