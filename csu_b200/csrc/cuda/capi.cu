@@ -209,6 +209,7 @@ static void plan(csu_ctx* x, Arena& a)
     x->d_prm = carve<Prm>(a, x->nsolve);
     s.dbg_ghost = carve<double>(a, (size_t)(nb > 0 ? nb : 1) * (nv + 1));
     s.lsq_x87 = carve<unsigned long long>(a, 1);
+    s.dQ = x->cfg.sst && x->cfg.time_scheme == CSU_TS_LUSGS ? carve<double>(a, (size_t)6 * nc) : nullptr;
     s.gfix = carve<int2>(a, (size_t)nc * (nv + 1)); // at most one entry per cell and variable (and T)
     s.gfix_n = carve<unsigned>(a, 2);
     if (!x->is_pack) {
@@ -451,17 +452,14 @@ static int validate_config(const char* who, const csu_config* cfg, int* model_ou
         csu_set_error("%s: nvar %d does not match the turbulence model", who, cfg->nvar);
         return CSU_ERR_INPUT;
     }
-    if (model == 2 && (cfg->flux == CSU_FLUX_ROE || cfg->sst_trans || cfg->time_scheme != CSU_TS_RK)) {
-        csu_set_error("%s: SST supports RK time stepping with the AUSM family (the reference has no Roe "
-                      "branch for SST and calls 4x4 DPLUR blocks with 6 variables); sstTrans not yet available", who);
+    if (model == 2 && (cfg->flux == CSU_FLUX_ROE || cfg->sst_trans || cfg->time_scheme == CSU_TS_DPLUR)) {
+        csu_set_error("%s: SST supports RK and LU-SGS time stepping with the AUSM family (the reference has no "
+                      "Roe branch for SST and calls 4x4 DPLUR blocks with 6 variables); sstTrans not yet available",
+                      who);
         return CSU_ERR_UNSUPPORTED;
     }
     if (model == 1 && cfg->sa_cc) {
         csu_set_error("%s: saCC is not available in this engine build", who);
-        return CSU_ERR_UNSUPPORTED;
-    }
-    if (cfg->time_scheme == CSU_TS_LUSGS && model == 2) {
-        csu_set_error("%s: LU-SGS with SST is not available in this engine build", who);
         return CSU_ERR_UNSUPPORTED;
     }
     if (cfg->time_scheme == CSU_TS_RK && !(cfg->stages >= 1 && cfg->stages <= 5)) {
@@ -565,6 +563,11 @@ extern "C" int csu_create(const csu_mesh_desc* md, const csu_config* cfg, csu_ct
     x->cfg = *cfg;
     st = csu_layout_build(md, cfg->axisymmetric, &x->L);
     if (!st && cfg->gradient == 1) st = csu_layout_green_gauss(&x->L);
+    {
+        // CSU_LUSGS_ORDER=sequential: LU-SGS in the reference's cell order (one cell per colour), for checks
+        const char* ord = getenv("CSU_LUSGS_ORDER");
+        if (!st && ord && strcmp(ord, "sequential") == 0) st = csu_layout_sequential_colors(&x->L);
+    }
     if (st) {
         delete x;
         csu_set_error("csu_create: mesh layout failed (a cell with more than four faces?)");
@@ -1213,6 +1216,16 @@ extern "C" int csu_dump(csu_ctx* x, int what, double* out)
             for (int j = 0; j < 4; j++)
                 for (size_t e = 0; e < per; e++) o[j * per + e] = a[((size_t)j * per + e) * nc + c];
         }
+        return CSU_OK;
+    }
+    case CSU_DUMP_SST_JAC: {
+        if (!x->st.dQ) {
+            csu_set_error("csu_dump: no SST source Jacobians in this context (SST with LU-SGS only)");
+            return CSU_ERR_STATE;
+        }
+        CK(d2h(a, x->st.dQ, (size_t)6 * nc));
+        for (int q = 0; q < 6; q++)
+            for (int c = 0; c < nc; c++) out[(size_t)q * nc + n2o[c]] = a[(size_t)q * nc + c];
         return CSU_OK;
     }
     case CSU_DUMP_LSQ_X87: {

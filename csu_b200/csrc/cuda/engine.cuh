@@ -138,6 +138,7 @@ struct State {
     const int* csolve;                        // packs: solve of each cell (null: one solve)
     double* dbg_ghost;                        // optional: ghost primitives [bface][NP] (reference order)
     unsigned long long* lsq_x87;              // running count of gradient slots left to the integer x87 model
+    double* dQ;                               // SST LU-SGS: source Jacobians [6][cell] (sst_source_jacobians)
     int2* gfix;                               // gradient variables left to k_grad_fix: (cell, var | mask << 8)
     unsigned* gfix_n;                         // [0] entries in gfix, [1] k_grad_fix blocks done (both reset
                                               // by the last block of k_grad_fix)

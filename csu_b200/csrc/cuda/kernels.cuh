@@ -871,6 +871,18 @@ __global__ void __launch_bounds__(BLOCK) k_impl(const Prm* __restrict__ P, const
         if (WITH_R) {
             gather_residual<MODEL>(p, m, s, c, P, R);
             storeR<MODEL>(s, nc, c, R);
+            if constexpr (MODEL == 2) {
+                // the SST source Jacobians of the LU-SGS diagonal (sstInterSource, sst.c:643-680)
+                if (s.dQ) {
+                    double4 gx = s.G4x[c], gy = s.G4y[c];
+                    double sgx[4] = {gx.y, gx.z, s.Gxx[c], s.Gxx[(size_t)nc + c]};
+                    double sgy[4] = {gy.y, gy.z, s.Gxy[c], s.Gxy[(size_t)nc + c]};
+                    double J[6];
+                    sst_source_jacobians(p.sst_k, sgx, sgy, P, m.wall_d[c], m.omega[c], J);
+#pragma unroll
+                    for (int q = 0; q < 6; q++) s.dQ[(size_t)q * nc + c] = J[q];
+                }
+            }
         }
         const int ni = m.nint[c], ns = m.nslot[c];
         double Lc = 0, Lv = 0;
@@ -1150,11 +1162,13 @@ __device__ __forceinline__ void delta_flux(const Prm& p, const double* P, const 
     double T = pr / (p.gas.R * rho);
     double e0 = T2e(p.gas, T);
     double E = e0 + (u * u + v * v) / 2;
+    if constexpr (MODEL == 2) E = E + P[5]; // implicitCalcDeltaFlux_sst (implicit.c:1048-1118): + k
     U[0] = rho;
     U[1] = rho * u;
     U[2] = rho * v;
     U[3] = rho * E;
-    if constexpr (MODEL == 1) U[4] = rho * P[5];
+    if constexpr (MODEL >= 1) U[4] = rho * P[5];
+    if constexpr (MODEL == 2) U[5] = rho * P[6];
     aux_flux<NV>(U, pr, nx, ny, F0);
 #pragma unroll
     for (int k = 0; k < NV; k++) U[k] = U[k] + d[k];
@@ -1165,6 +1179,33 @@ __device__ __forceinline__ void delta_flux(const Prm& p, const double* P, const 
         E = U[3] / rho;
         double e1 = E - 0.5 * (u * u + v * v);
         T = e2Taprox(p.gas, e0, T, e1);
+        pr = p.gas.R * T * rho;
+    } else if constexpr (MODEL == 2) {
+        rho = U[0];
+        rho = fmax(rho, p.r_lim);
+        U[0] = rho;
+        u = U[1] / rho;
+        v = U[2] / rho;
+        double k = U[4] / rho;
+        if (k < 1e-14) {
+            k = 1e-14;
+            U[4] = rho * k;
+        }
+        double om = U[5] / rho;
+        if (om < 0.0) { // omLim = 0 (solver.c:1155)
+            om = 0.0;
+            U[5] = rho * om;
+        }
+        E = U[3] / rho;
+        double e1 = E - (u * u + v * v) * 0.5 - k;
+        e1 = fmax(e1, 7.176325e+02);
+        T = e2Taprox(p.gas, e0, T, e1);
+        if (T < 1) {
+            T = 1;
+            e1 = T2e(p.gas, T);
+            E = e1 + (u * u + v * v) * 0.5 + k;
+            U[3] = rho * E;
+        }
         pr = p.gas.R * T * rho;
     } else {
         rho = U[0];
@@ -1230,6 +1271,17 @@ __global__ void __launch_bounds__(BLOCK) k_lusgs(const Prm* __restrict__ P, cons
         x[0] = D * t4.x; x[1] = D * t4.y; x[2] = D * t4.z; x[3] = D * t4.w;
 #pragma unroll
         for (int k = 4; k < NV; k++) x[k] = D * s.Xx[0][(size_t)(k - 4) * nc + c];
+        if constexpr (MODEL == 2) {
+            // implicitLUSGS_U (implicit.c:372-390): the k, omega rows multiply by the SST diagonal block
+            const double x0 = t4.x, x4 = s.Xx[0][c], x5 = s.Xx[0][(size_t)nc + c];
+            const double a = D - s.dQ[(size_t)nc + c], b = -s.dQ[(size_t)2 * nc + c];
+            const double cq = -s.dQ[(size_t)4 * nc + c], dq = D - s.dQ[(size_t)5 * nc + c];
+            const double det = a * dq - b * cq;
+            if (!(fabs(det) < 1e-14)) {
+                x[4] = a * x4 + b * x5 - s.dQ[c] * x0;
+                x[5] = cq * x4 + dq * x5 - s.dQ[(size_t)3 * nc + c] * x0;
+            }
+        }
     }
     double P0[NP];
     loadP<MODEL>(s, nc, c, P0);
@@ -1256,7 +1308,8 @@ __global__ void __launch_bounds__(BLOCK) k_lusgs(const Prm* __restrict__ P, cons
         delta_flux<MODEL>(p, Pn, dn, nx, ny, dF);
         double cc = T2c(p.gas, Pn[4]);
         double ra = p.w_imp * (fabs(nx * Pn[1] + ny * Pn[2]) + cc) * dS;
-        if constexpr (MODEL == 1) {
+        if constexpr (MODEL >= 1) {
+            // implicitFunc_sa / implicitFunc_sst (implicit.c:560-567, 1140-1150): the face eddy viscosity
             double r = Pn[0], T = Pn[4];
             double mi = sutherland(T);
             ra += fmax(4 / (3 * r), T2gamma(p.gas, T) / r) * (mi / p.pr + s.MIT[f] / p.pr_t) * dS / m.fL[f];
@@ -1266,8 +1319,37 @@ __global__ void __launch_bounds__(BLOCK) k_lusgs(const Prm* __restrict__ P, cons
 #pragma unroll
         for (int k = 0; k < NV; k++) x[k] -= 0.5 * (dF[k] * dS - ra * dn[k]);
     }
+    if constexpr (MODEL == 2) {
+        // the SST diagonal (implicit.c:323-345, 444-465): D on the mean flow, a 2x2 block with the source
+        // Jacobians on k and omega, its determinant in double and the quotients in long double
 #pragma unroll
-    for (int k = 0; k < NV; k++) x[k] /= D;
+        for (int k = 0; k < 4; k++) x[k] /= D;
+        const double A = x[4] + s.dQ[c] * x[0];
+        const double B = x[5] + s.dQ[(size_t)3 * nc + c] * x[0];
+        const double a = D - s.dQ[(size_t)nc + c], b = -s.dQ[(size_t)2 * nc + c];
+        const double cq = -s.dQ[(size_t)4 * nc + c], dq = D - s.dQ[(size_t)5 * nc + c];
+        const double det = a * dq - b * cq;
+        if (fabs(det) < 1e-14) {
+            x[4] /= D;
+            x[5] /= D;
+        } else {
+            const double n4 = A * dq - B * b, n5 = -A * cq + B * a;
+            bool ok = true;
+            const double q4 = x87_div_d(n4, det, ok);
+            const double q5 = x87_div_d(n5, det, ok);
+            if (ok) {
+                x[4] = q4;
+                x[5] = q5;
+            } else {
+                const X80 dx = x80_from_double(det);
+                x[4] = x80_to_double(x80_div(x80_from_double(n4), dx));
+                x[5] = x80_to_double(x80_div(x80_from_double(n5), dx));
+            }
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < NV; k++) x[k] /= D;
+    }
     double4* dst4 = FWD ? s.X4[0] : s.X4[1];
     double* dstx = FWD ? s.Xx[0] : s.Xx[1];
     dst4[c] = make_double4(x[0], x[1], x[2], x[3]);

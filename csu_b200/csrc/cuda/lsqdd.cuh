@@ -221,6 +221,24 @@ X80_HD DD x87_add(DD a, DD b, bool& ok)
     return x87_round(v.h, r, fabs(t.l), ok);
 }
 
+// The double a `long double` division of two doubles stores, RN53(RN64(n / d)) (the reference's SST
+// diagonal solves, implicit.c:341-342): h = RN53(n / d) with its exact remainder gives the quotient as a
+// double-double to ~2^-106, rounded on the 64-bit grid (bound 2^-100 |h|); its high part is the store.
+// ok is cleared when that rounding cannot be decided (or for zero, non-finite and extreme quotients).
+X80_HD double x87_div_d(double n, double d, bool& ok)
+{
+    double h = n / d;
+    if (n == 0.0) return h; // +-0 in x87 as in double
+    if (h == 0.0 || !(fabs(h) <= 1.7976931348623157e308)) {
+        ok = false;
+        return h;
+    }
+    double r = fma(-h, d, n); // n - h d exactly
+    DD t = {r / d, 0.0};
+    DD q64 = x87_round(h, t, 0x1p-100 * fabs(h), ok);
+    return q64.h;
+}
+
 // q as the double RN53(q) if [q - E, q + E] holds no rounding boundary of double precision.
 X80_HD bool dd_round_certified(DD q, double E, double* out)
 {

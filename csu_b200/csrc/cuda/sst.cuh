@@ -289,4 +289,50 @@ __device__ __forceinline__ void sst_cell_source(const SstK& c, const double* gx,
     *Qto = v.Qto;
 }
 
+// sstInterSource's source Jacobians for LU-SGS (sst.c:643-680): forward differences of Qtk, Qto in omega,
+// k and rho (step max(|x| 1e-6, 1e-6), the variable record reused between evaluations as there), combined
+// into derivatives with respect to rho, rho k and rho omega and multiplied by the cell area. J: dQk/dr,
+// dQk/d(rk), dQk/d(ro), dQo/dr, dQo/d(rk), dQo/d(ro); all zero when omega sits at its lower limit 0.
+__device__ __forceinline__ void sst_source_jacobians(const SstK& c, const double* gx, const double* gy,
+                                                     const double* P, double d, double area, double* J)
+{
+    SstVar v;
+    v.dux = gx[0]; v.dvx = gx[1]; v.dkx = gx[2]; v.dox = gx[3];
+    v.duy = gy[0]; v.dvy = gy[1]; v.dky = gy[2]; v.doy = gy[3];
+    v.r = P[0];
+    v.T = P[4];
+    v.k = P[5];
+    v.om = P[6];
+    v.d = d;
+    v.mi_L = sutherland(v.T);
+    if (v.om == 0.0) {
+        for (int q = 0; q < 6; q++) J[q] = 0.0;
+        return;
+    }
+    sst_sources(c, v);
+    const double Qk0 = v.Qtk, Qo0 = v.Qto;
+    const double h = 1e-6, dh = 1e-6;
+    double hh = fmax(fabs(v.om * h), dh);
+    v.om += hh;
+    sst_sources(c, v);
+    const double dQkdo = (v.Qtk - Qk0) / hh, dQodo = (v.Qto - Qo0) / hh;
+    v.om = P[6];
+    hh = fmax(fabs(v.k * h), dh);
+    v.k += hh;
+    sst_sources(c, v);
+    const double dQkdk = (v.Qtk - Qk0) / hh, dQodk = (v.Qto - Qo0) / hh;
+    v.k = P[5];
+    hh = fmax(fabs(v.r * h), dh);
+    v.r += hh;
+    sst_sources(c, v);
+    const double dQkdr = (v.Qtk - Qk0) / hh, dQodr = (v.Qto - Qo0) / hh;
+    v.r = P[0];
+    J[0] = (dQkdr - dQkdk * v.k / v.r - dQkdo * v.om / v.r) * area;
+    J[1] = dQkdk * area / v.r;
+    J[2] = dQkdo * area / v.r;
+    J[3] = (dQodr - dQodk * v.k / v.r - dQodo * v.om / v.r) * area;
+    J[4] = dQodk * area / v.r;
+    J[5] = dQodo * area / v.r;
+}
+
 } // namespace csu

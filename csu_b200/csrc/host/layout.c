@@ -121,6 +121,29 @@ void csu_layout_free(csu_layout* L)
     memset(L, 0, sizeof(*L));
 }
 
+int csu_layout_sequential_colors(csu_layout* L)
+{
+    const int nc = L->nc;
+    int* start = malloc(sizeof(int) * (nc + 1));
+    int* cells = malloc(sizeof(int) * (nc > 0 ? nc : 1));
+    if (!start || !cells) {
+        free(start);
+        free(cells);
+        return CSU_ERR_OOM;
+    }
+    for (int c = 0; c < nc; c++) {
+        L->color[c] = L->cell_new2old[c];
+        cells[L->cell_new2old[c]] = c;
+    }
+    for (int k = 0; k <= nc; k++) start[k] = k;
+    free(L->color_start);
+    free(L->color_cells);
+    L->color_start = start;
+    L->color_cells = cells;
+    L->ncolors = nc;
+    return CSU_OK;
+}
+
 int csu_layout_build(const csu_mesh_desc* m, int axi, csu_layout* L)
 {
     memset(L, 0, sizeof(*L));

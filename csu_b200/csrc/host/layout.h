@@ -90,6 +90,9 @@ typedef struct csu_layout {
 int csu_layout_build(const csu_mesh_desc* m, int axi, csu_layout* L);
 void csu_layout_free(csu_layout* L);
 int csu_layout_green_gauss(csu_layout* L);
+/* LU-SGS colouring with one cell per colour in the reference's cell order: the multicolour sweeps then
+   visit cells exactly as implicitLUSGS_L / _U do (implicit.c:274-482), one launch per cell (for checks) */
+int csu_layout_sequential_colors(csu_layout* L);
 
 #ifdef __cplusplus
 }

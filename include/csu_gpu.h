@@ -188,7 +188,9 @@ int csu_tube_run(csu_ctx* ctx, double tmax, int* steps, double* t_final);
  *  CSU_DUMP_BLOCKS  ncells*4*nvar*nvar          DPLUR blocks [cell][slot][row][col], slots in ELEMENT.f order
  *  CSU_DUMP_LSQ_X87 1                           gradient slots (cell, variable) so far that the FP64
  *                                               least squares could not decide and left to the integer x87
- *                                               model (no reference counterpart: a diagnostic of this engine) */
+ *                                               model (no reference counterpart: a diagnostic of this engine)
+ *  CSU_DUMP_SST_JAC 6*ncells                    SST source Jacobians dQkdr, dQkdrk, dQkdro, dQodr, dQodrk,
+ *                                               dQodro [6][cell] of the last LU-SGS iteration (sst.c:643-680) */
 #define CSU_DUMP_P 1
 #define CSU_DUMP_GHOST_P 2
 #define CSU_DUMP_GRAD 3
@@ -200,6 +202,7 @@ int csu_tube_run(csu_ctx* ctx, double tmax, int* steps, double* t_final);
 #define CSU_DUMP_DW 9
 #define CSU_DUMP_BLOCKS 10
 #define CSU_DUMP_LSQ_X87 11
+#define CSU_DUMP_SST_JAC 12
 int csu_dump(csu_ctx* ctx, int what, double* out);
 
 /* Run the engine's work on a caller-provided cudaStream_t (NULL: the context's own stream). */

@@ -188,6 +188,15 @@ void ref_calc_R(void)
     solverCalcR(g, g->U);
 }
 
+/* the SST source Jacobians of the last solverCalcR (sstInterSource): dQkdr, dQkdrk, dQkdro, dQodr, dQodrk,
+   dQodro, [6][cell] */
+void ref_sst_jac(double* J)
+{
+    const int n = g->mesh->Nelem;
+    const double* a[6] = {g->dQkdr, g->dQkdrk, g->dQkdro, g->dQodr, g->dQodrk, g->dQodro};
+    for (int q = 0; q < 6; q++) memcpy(J + (size_t)q * n, a[q], sizeof(double) * n);
+}
+
 void ref_get_R(double* R)
 {
     for (int k = 0; k < g->Nvar; k++)

@@ -102,6 +102,12 @@ class Ref:
         dt = self.L.ref_calc_dt(_p(dtl))
         return dt, dtl
 
+    def sst_jac(self):
+        """SST source Jacobians of the last calc_R, [6][cell]."""
+        J = np.zeros(6 * self.nc)
+        self.L.ref_sst_jac(_p(J))
+        return J.reshape(6, self.nc)
+
     def implicit_D(self):
         D, dtl = np.zeros(self.nc), np.zeros(self.nc)
         self.L.ref_implicit_D(_p(D), _p(dtl))
