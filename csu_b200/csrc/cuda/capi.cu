@@ -33,6 +33,12 @@ const double RK5[5] = {0.0533, 0.1263, 0.2375, 0.4414, 1.0};
 
 } // namespace
 
+// DPLUR sweeps run in blocks of SWEEP_BLOCK threads (more resident blocks per SM, finer waves); the first
+// sweep's partial norms then come one row per SWEEP_BLOCK cells.
+#ifndef SWEEP_BLOCK
+#define SWEEP_BLOCK 128
+#endif
+
 struct csu_ctx {
     int model = 0, nv = 4;
     csu_config cfg;
@@ -201,7 +207,8 @@ static void plan(csu_ctx* x, Arena& a)
     bool dplur = x->cfg.time_scheme == CSU_TS_DPLUR;
     s.blocks = dplur && !x->cfg.implicit_fp32 ? carve<double>(a, c4 * nv * nv) : nullptr;
     s.blocks32 = dplur && x->cfg.implicit_fp32 ? carve<float>(a, c4 * nv * nv) : nullptr;
-    s.part = carve<double>(a, (size_t)((nc + BLOCK - 1) / BLOCK) * nv);
+    // partial norms: one row per 256-cell block, or per 128-cell block from the DPLUR first sweep
+    s.part = carve<double>(a, (size_t)((nc + BLOCK - 1) / BLOCK) * (BLOCK / SWEEP_BLOCK) * nv);
     s.bcoef = carve<double>(a, (size_t)4 * (nb > 0 ? nb : 1));
     s.sc = carve<Scalars>(a, x->nsolve);
     s.bsolve = x->nsolve > 1 ? carve<int>(a, (nc + BLOCK - 1) / BLOCK) : nullptr;
@@ -779,7 +786,8 @@ static void launch_flux(csu_ctx* x, int coef)
 template <int MODEL>
 static void launch_finalize(csu_ctx* x, int mode)
 {
-    k_finalize<MODEL><<<x->nsolve, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st, mode);
+    const int ppb = x->cfg.time_scheme == CSU_TS_DPLUR && mode == 1 ? BLOCK / SWEEP_BLOCK : 1;
+    k_finalize<MODEL><<<x->nsolve, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st, mode, ppb);
     x->launches++;
     tmark(x, KFIN);
 }
@@ -816,17 +824,13 @@ static void launch_blocks(csu_ctx* x)
     else cudaEventRecord(x->ev_join, x->side);
 }
 
-// Sweeps after the first run in blocks of SWEEP_BLOCK threads (more resident blocks per SM, finer waves).
-#ifndef SWEEP_BLOCK
-#define SWEEP_BLOCK 128
-#endif
 template <int MODEL>
 static void launch_sweep(csu_ctx* x, int m, int n)
 {
     constexpr int SB = SWEEP_BLOCK;
     if (m == 0) {
-        auto* k = m == n - 1 ? k_sweep<MODEL, true, true, BLOCK> : k_sweep<MODEL, false, true, BLOCK>;
-        k<<<x->gb_c, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st, m, x->xcur);
+        auto* k = m == n - 1 ? k_sweep<MODEL, true, true, SB> : k_sweep<MODEL, false, true, SB>;
+        k<<<x->gb_c * (BLOCK / SB), SB, 0, x->stream>>>(x->d_prm, x->mesh, x->st, m, x->xcur);
     } else {
         auto* k = m == n - 1 ? k_sweep<MODEL, true, false, SB> : k_sweep<MODEL, false, false, SB>;
         k<<<x->gb_c * (BLOCK / SB), SB, 0, x->stream>>>(x->d_prm, x->mesh, x->st, m, x->xcur);

@@ -454,8 +454,8 @@ __device__ __forceinline__ double block_max(double v)
 }
 
 // Block-wide sums of N values per thread; result valid in thread 0. Deterministic order.
-template <int N>
-__device__ __forceinline__ void block_sum(double* v, double (*sh)[BLOCK / 32])
+template <int N, int NT = BLOCK>
+__device__ __forceinline__ void block_sum(double* v, double (*sh)[NT / 32])
 {
     int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
 #pragma unroll
@@ -468,7 +468,7 @@ __device__ __forceinline__ void block_sum(double* v, double (*sh)[BLOCK / 32])
 #pragma unroll
         for (int k = 0; k < N; k++) {
             double acc = 0.0;
-            for (int j = 0; j < BLOCK / 32; j++) acc += sh[k][j];
+            for (int j = 0; j < NT / 32; j++) acc += sh[k][j];
             v[k] = acc;
         }
     }

@@ -753,15 +753,17 @@ __device__ __forceinline__ void storeR(const State& s, int nc, int c, const doub
     for (int k = 4; k < Model<MODEL>::NV; k++) s.Rx[(size_t)(k - 4) * nc + c] = R[k];
 }
 
-template <int MODEL>
+// the block's sum of R^2 per variable into s.part[blockIdx.x]: one row per cell block of NT cells (k_finalize
+// is told how many rows a BLOCK-cell block has)
+template <int MODEL, int NT = BLOCK>
 __device__ __forceinline__ void partial_norms(const State& s, bool valid, const double* R)
 {
     constexpr int NV = Model<MODEL>::NV;
-    __shared__ double sh[NV][BLOCK / 32];
+    __shared__ double sh[NV][NT / 32];
     double v[NV];
 #pragma unroll
     for (int k = 0; k < NV; k++) v[k] = valid ? R[k] * R[k] : 0.0;
-    block_sum<NV>(v, sh);
+    block_sum<NV, NT>(v, sh);
     if (threadIdx.x == 0)
         for (int k = 0; k < NV; k++) s.part[(size_t)blockIdx.x * NV + k] = v[k];
 }
@@ -1043,7 +1045,7 @@ __global__ void __launch_bounds__(SB) k_sweep(const Prm* __restrict__ P, const _
                                               const __grid_constant__ State s, int sweep, int cur)
 {
     constexpr int NV = Model<MODEL>::NV, NP = Model<MODEL>::NP;
-    static_assert(BLOCK % SB == 0 && (!FIRST || SB == BLOCK), "sweep blocks tile the cell blocks");
+    static_assert(BLOCK % SB == 0, "sweep blocks tile the cell blocks");
     // SB-thread blocks: BLOCK / SB of them cover one cell block of the solve map
     const int sid = s.bsolve ? s.bsolve[blockIdx.x / (BLOCK / SB)] : 0;
     const Prm& p = P[sid];
@@ -1147,7 +1149,7 @@ __global__ void __launch_bounds__(SB) k_sweep(const Prm* __restrict__ P, const _
         double v = block_max<SB>(dmax);
         if (threadIdx.x == 0) atomicMax(&sc->sweep_max[sweep], dbits(v));
     }
-    if (FIRST) partial_norms<MODEL>(s, valid, R);
+    if (FIRST) partial_norms<MODEL, SB>(s, valid, R);
 }
 
 // implicitCalcDeltaFlux (implicit.c:194-231) and implicitCalcDeltaFlux_sa (495-552): F(U + d) - F(U) on the
@@ -1386,15 +1388,16 @@ __global__ void __launch_bounds__(BLOCK) k_update(const Prm* __restrict__ P, con
 // ------------------------------------------------------------------------------------------------
 template <int MODEL>
 __global__ void __launch_bounds__(BLOCK) k_finalize(const Prm* __restrict__ P, const __grid_constant__ Mesh m,
-                                                    const __grid_constant__ State s, int mode)
+                                                    const __grid_constant__ State s, int mode, int ppb)
 {
     constexpr int NV = Model<MODEL>::NV;
     __shared__ double sh[NV + 4][BLOCK / 32];
     const int sid = blockIdx.x; // one block per solve
     const Prm& p = P[sid];
     Scalars* const sc = s.sc + sid;
-    const int npart = p.nblk, nwall = p.nwall;
-    const double* part = s.part + (size_t)p.blk0 * NV;
+    // ppb rows of partial norms per cell block (the DPLUR first sweep writes one per 128 cells)
+    const int npart = p.nblk * ppb, nwall = p.nwall;
+    const double* part = s.part + (size_t)p.blk0 * ppb * NV;
     const double* bcoef = s.bcoef + (size_t)p.wall0 * 4;
     // Everything the block reads is requested before the halted test, so the loads overlap: a chain of
     // dependent round trips to the L2 would be most of a one-block kernel's time. Thread 0 keeps a copy of
