@@ -376,6 +376,7 @@ static void fill_params_from(const csu_config& c, const csu_layout& L, Prm& p)
         k.g1 = k.b1 / k.bs - k.so1 * kap * kap / sqrt(k.bs);
         k.g2 = k.b2 / k.bs - k.so2 * kap * kap / sqrt(k.bs);
         k.o_wall_factor = c.o_wall_factor;
+        k.trans = c.sst_trans ? 1 : 0;
     }
     p.o_wall_factor = c.o_wall_factor;
     p.tmax = 0;
@@ -459,10 +460,9 @@ static int validate_config(const char* who, const csu_config* cfg, int* model_ou
         csu_set_error("%s: nvar %d does not match the turbulence model", who, cfg->nvar);
         return CSU_ERR_INPUT;
     }
-    if (model == 2 && (cfg->flux == CSU_FLUX_ROE || cfg->sst_trans || cfg->time_scheme == CSU_TS_DPLUR)) {
+    if (model == 2 && (cfg->flux == CSU_FLUX_ROE || cfg->time_scheme == CSU_TS_DPLUR)) {
         csu_set_error("%s: SST supports RK and LU-SGS time stepping with the AUSM family (the reference has no "
-                      "Roe branch for SST and calls 4x4 DPLUR blocks with 6 variables); sstTrans not yet available",
-                      who);
+                      "Roe branch for SST and calls 4x4 DPLUR blocks with 6 variables)", who);
         return CSU_ERR_UNSUPPORTED;
     }
     if (model == 1 && cfg->sa_cc) {

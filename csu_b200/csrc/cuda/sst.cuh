@@ -10,6 +10,7 @@ namespace csu {
 // constants of sstInit (sst.c:18-39); g1, g2 evaluated on the host with the reference's expressions
 struct SstK {
     double sk1, so1, b1, sk2, so2, b2, bs, a1, g1, g2, o_wall_factor;
+    int trans; // sstTrans 1: the low-Reynolds variant of sstTrans.c (sstTransFlux, sstTransSources)
 };
 
 struct SstVar {
@@ -46,9 +47,96 @@ __device__ __forceinline__ double sst_F2(double n_L_term, double sqrtk_term)
     return tanh(arg2 * arg2);
 }
 
+// The sstTrans variant (sstTrans.c; constants of sstTransInit, lines 18-35, equal to sstInit's where the
+// names agree: sk1 so1 b1 sk2 so2 b2, bs2 = bs, a1). Its Reynolds numbers are fixed at Ry = Rt = 1e6.
+// sstTransF1 (sstTrans.c:120-139) is sstF1 without the omega = 0 guard.
+__device__ __forceinline__ double sst_trans_F1(const SstK& c, const SstVar& v, double n_L_term, double sqrtk_term)
+{
+    double aux1, aux2;
+    aux1 = 2 * v.r * c.so2 * (v.dkx * v.dox + v.dky * v.doy) / v.om;
+    double CD = fmax(aux1, 1.0e-20);
+    aux1 = sqrtk_term;
+    aux2 = n_L_term;
+    aux1 = fmax(aux1, aux2);
+    aux2 = 4 * v.r * c.so2 * v.k / (CD * v.d * v.d);
+    double arg1 = fmin(aux1, aux2);
+    return tanh(arg1 * arg1 * arg1 * arg1);
+}
+
+// the blend factor F1 of the variant: max(F1s, exp(-(Ry / 120)^8)) (sstTrans.c:57-64, 146-153)
+__device__ __forceinline__ double sst_trans_blend_F1(const SstK& c, const SstVar& v, double n_L_term,
+                                                     double sqrtk_term)
+{
+    double Fs1 = sst_trans_F1(c, v, n_L_term, sqrtk_term);
+    double Ry = 1e6;
+    double aux = Ry / 120;
+    aux = aux * aux;
+    aux = aux * aux;
+    aux = aux * aux;
+    return fmax(Fs1, exp(-aux));
+}
+
+// sstTransFlux (sstTrans.c:42-81)
+__device__ __forceinline__ void sst_trans_flux(const SstK& c, SstVar& v)
+{
+    double n_L = v.mi_L / v.r;
+    double omega = fabs(v.duy - v.dvx);
+    double sqrtk = sqrt(v.k);
+    double sqrtk_term = sqrtk / (c.bs * v.om * v.d);
+    double n_L_term = 500 * n_L / (v.d * v.d * v.om);
+    double F1 = sst_trans_blend_F1(c, v, n_L_term, sqrtk_term);
+    double F2 = sst_F2(n_L_term, sqrtk_term);
+    double Rt = 1e6;
+    double alphas1 = (.025 + Rt / 6) / (1 + Rt / 6);
+    double alphas = sst_blend(alphas1, 1.0, F1);
+    double sk = sst_blend(c.sk1, c.sk2, F1);
+    double so = sst_blend(c.so1, c.so2, F1);
+    v.mi_t = fmin(alphas * v.r * v.k / v.om, c.a1 * v.r * v.k / (omega * F2));
+    double aux = (v.mi_L + sk * v.mi_t);
+    v.tkx = aux * v.dkx;
+    v.tky = aux * v.dky;
+    aux = (v.mi_L + so * v.mi_t);
+    v.tox = aux * v.dox;
+    v.toy = aux * v.doy;
+}
+
+// sstTransSources (sstTrans.c:141-174, with sstTransAlpha1 / Alphas1 / Bs1)
+__device__ __forceinline__ void sst_trans_sources(const SstK& c, SstVar& v)
+{
+    double n_L = v.mi_L / v.r;
+    double omega = fabs(v.duy - v.dvx);
+    double sqrtk = sqrt(v.k);
+    double sqrtk_term = sqrtk / (c.bs * v.om * v.d);
+    double n_L_term = 500 * n_L / (v.d * v.d * v.om);
+    double F1 = sst_trans_blend_F1(c, v, n_L_term, sqrtk_term);
+    double F2 = sst_F2(n_L_term, sqrtk_term);
+    double Rt = 1e6;
+    double alpha1 = (5. / 9.) * (0.1 + Rt / 2.7) / (1 + Rt / 2.7);
+    double alphas1 = (.025 + Rt / 6) / (1 + Rt / 6);
+    double a8 = Rt / 8;
+    a8 = a8 * a8;
+    a8 = a8 * a8;
+    double bs1 = 0.09 * (5. / 18. + a8) / (1 + a8);
+    double alpha = sst_blend(alpha1, 0.4403, F1);
+    double alphas = sst_blend(alphas1, 1.0, F1);
+    double b = sst_blend(c.b1, c.b2, F1);
+    double bs = sst_blend(bs1, c.bs, F1);
+    v.mi_t = fmin(alphas * v.r * v.k / v.om, c.a1 * v.r * v.k / (omega * F2));
+    double n_t = v.mi_t / v.r;
+    double P = v.mi_t * omega * omega;
+    v.F1 = F1;
+    v.F2 = F2;
+    v.Qtk = P - bs * v.r * v.om * v.k;
+    v.Qto = alpha * P / n_t - b * v.r * v.om * v.om + 2 * (1 - F1) * v.r * c.so2 * (v.dkx * v.dox + v.dky * v.doy) / v.om;
+}
+
 // sstFlux (sst.c:749-786): eddy viscosity and the k, omega diffusion fluxes
 __device__ __forceinline__ void sst_flux(const SstK& c, SstVar& v)
 {
+    if (c.trans) {
+        sst_trans_flux(c, v);
+        return;
+    }
     double n_L = v.mi_L / v.r;
     double omega = fabs(v.duy - v.dvx);
     double sqrtk_term = sqrt(v.k) / (c.bs * v.om * v.d);
@@ -70,6 +158,10 @@ __device__ __forceinline__ void sst_flux(const SstK& c, SstVar& v)
 // sstSources (sst.c:698-747): Qtk, Qto per unit volume
 __device__ __forceinline__ void sst_sources(const SstK& c, SstVar& v)
 {
+    if (c.trans) {
+        sst_trans_sources(c, v);
+        return;
+    }
     double n_L = v.mi_L / v.r;
     double omega = fabs(v.duy - v.dvx);
     double sqrtk_term = sqrt(v.k) / (c.bs * v.om * v.d);

@@ -1,6 +1,7 @@
-"""Menter SST path (sst.c) vs the reference. The reference ships no SST case; its SA flat plate
-(caseBL_turb) is run with `sst, 1` instead (RK: the reference's SST DPLUR multiplies 4x4 blocks into
-6 variables, implicit.c:993-1000 with 938-972, so only the explicit path has defined results)."""
+"""Menter SST path (sst.c) vs the reference, and its sstTrans variant (sstTrans.c). The reference ships no
+SST case; its SA flat plate (caseBL_turb) is run with `sst, 1` instead (RK here; LU-SGS in
+test_gpu_lusgs_seq.py; the reference's SST DPLUR multiplies 4x4 blocks into 6 variables,
+implicit.c:993-1000 with 938-972, so it has no defined results)."""
 import numpy as np
 import pytest
 
@@ -20,8 +21,9 @@ def _setup(kv=None):
     return csu_b200.Engine(case), case, Ref(wd)
 
 
-def test_sst_residual(native):
-    eng, case, ref = _setup()
+@pytest.mark.parametrize("trans", ["0", "1"], ids=["sst", "sstTrans"])
+def test_sst_residual(native, trans):
+    eng, case, ref = _setup({"sstTrans": trans})
     ref.iterate(3)
     U = ref.get_U()
     eng.set_state(U)
@@ -32,10 +34,18 @@ def test_sst_residual(native):
     diff = [int(np.count_nonzero(R[k] != R_ref[k])) for k in range(case.nvar)]
     print("SST: differing entries per variable %s of %d, max scaled err %.3e" % (diff, case.n_cells, err))
     assert err < 1e-12
+    if trans == "1":
+        # the variant's sources and diffusion differ from the standard model's on the same state
+        eng0, _, _ = _setup({"sstTrans": "0"})
+        eng0.set_state(U)
+        R0 = eng0.residual()
+        assert not np.array_equal(R0[4:], R[4:])
+        eng0.close()
 
 
-def test_sst_history(native):
-    eng, case, ref = _setup()
+@pytest.mark.parametrize("trans", ["0", "1"], ids=["sst", "sstTrans"])
+def test_sst_history(native, trans):
+    eng, case, ref = _setup({"sstTrans": trans})
     n = 10
     h_ref = ref.iterate(n)
     h = eng.iterate(n)
