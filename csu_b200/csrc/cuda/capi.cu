@@ -390,6 +390,7 @@ static void fill_params_from(const csu_config& c, const csu_layout& L, Prm& p)
     if ((lsq && !strcmp(lsq, "weights")) || (fast && fast[0] == '1')) p.lsq_exact = 0;
     p.visc = (c.laminar || c.sa || c.sst) ? 1 : 0;
     p.visc_blazek = c.visc_blazek;
+    p.sa_cc = c.sa_cc ? 1 : 0;
     p.conv_tol = c.conv_drop;
     p.iter_cap = c.iter_cap;
     p.lim_func = c.limiter_func;
@@ -463,10 +464,6 @@ static int validate_config(const char* who, const csu_config* cfg, int* model_ou
     if (model == 2 && (cfg->flux == CSU_FLUX_ROE || cfg->time_scheme == CSU_TS_DPLUR)) {
         csu_set_error("%s: SST supports RK and LU-SGS time stepping with the AUSM family (the reference has no "
                       "Roe branch for SST and calls 4x4 DPLUR blocks with 6 variables)", who);
-        return CSU_ERR_UNSUPPORTED;
-    }
-    if (model == 1 && cfg->sa_cc) {
-        csu_set_error("%s: saCC is not available in this engine build", who);
         return CSU_ERR_UNSUPPORTED;
     }
     if (cfg->time_scheme == CSU_TS_RK && !(cfg->stages >= 1 && cfg->stages <= 5)) {

@@ -7,6 +7,7 @@
 #include "lsqdd.cuh"
 #include "viscous.cuh"
 #include "sa.cuh"
+#include "sacc.cuh"
 #include "sst.cuh"
 
 namespace csu {
@@ -30,6 +31,7 @@ struct Prm {
                         // component, 2 certified double-double + x87 model for the rest (bit-exact)
     int visc;           // laminar, SA or SST: temperature gradient and viscous fluxes
     int visc_blazek;    // SA face gradients with the directional correction (saInterFaceB)
+    int sa_cc;          // saCC: SA with the density-gradient terms (saCC.c)
     double lim_k, vol_max, e_fix, r_lim, p_out, t_wall, pr, pr_t, w_imp, cfl, sigma, mach_inf, sref;
     double pin[7];
     double pref20[6];   // limiterUpdate type 0 reference squares (limiter.c:49-59)

@@ -555,12 +555,15 @@ __global__ void __launch_bounds__(FB) k_flux(const Prm* __restrict__ P, const __
             s.MIT[f] = mit;
         } else if constexpr (MODEL == 1) {
             double4 a = s.G4x[e.x], b = s.G4y[e.x], cc = s.G4x[e.y], d = s.G4y[e.y];
-            double g0x[4] = {a.y, a.z, s.GTx[e.x], s.Gxx[e.x]}, g0y[4] = {b.y, b.z, s.GTy[e.x], s.Gxy[e.x]};
-            double g1x[4] = {cc.y, cc.z, s.GTx[e.y], s.Gxx[e.y]}, g1y[4] = {d.y, d.z, s.GTy[e.y], s.Gxy[e.y]};
+            double g0x[5] = {a.y, a.z, s.GTx[e.x], s.Gxx[e.x], a.x}, g0y[5] = {b.y, b.z, s.GTy[e.x], s.Gxy[e.x], b.x};
+            double g1x[5] = {cc.y, cc.z, s.GTx[e.y], s.Gxx[e.y], cc.x}, g1y[5] = {d.y, d.z, s.GTy[e.y], s.Gxy[e.y], d.x};
             double2 dd = m.fd[f];
             double fv[4], mit;
-            sa_face_flux(p.gas, p.pr, p.pr_t, p.visc_blazek, g0x, g0y, g1x, g1y, A, B, dd.x, dd.y, m.fL[f], dSx,
-                         dSy, fv, &mit);
+            if (p.sa_cc)
+                sacc_face_flux(p.gas, p.pr, p.pr_t, g0x, g0y, g1x, g1y, A, B, dSx, dSy, fv, &mit);
+            else
+                sa_face_flux(p.gas, p.pr, p.pr_t, p.visc_blazek, g0x, g0y, g1x, g1y, A, B, dd.x, dd.y, m.fL[f], dSx,
+                             dSy, fv, &mit);
             s.FV[f] = make_double4(fv[0], fv[1], fv[2], fv[3]);
             s.MIT[f] = mit;
         } else if (p.laminar == 1) {
@@ -609,8 +612,8 @@ __global__ void __launch_bounds__(FB) k_flux(const Prm* __restrict__ P, const __
             gvy[0] = bb.y; gvy[1] = bb.z; gvy[2] = s.GTy[c];
             gvx[3] = MODEL >= 1 ? s.Gxx[c] : 0.0;
             gvy[3] = MODEL >= 1 ? s.Gxy[c] : 0.0;
-            gvx[4] = MODEL == 2 ? s.Gxx[(size_t)nc + c] : 0.0;
-            gvy[4] = MODEL == 2 ? s.Gxy[(size_t)nc + c] : 0.0;
+            gvx[4] = MODEL == 2 ? s.Gxx[(size_t)nc + c] : (MODEL == 1 ? a.x : 0.0); // SA: the rho gradient (saCC)
+            gvy[4] = MODEL == 2 ? s.Gxy[(size_t)nc + c] : (MODEL == 1 ? bb.x : 0.0);
             bdv = m.bd[b];
             bLv = m.bL[b];
         }
@@ -624,8 +627,12 @@ __global__ void __launch_bounds__(FB) k_flux(const Prm* __restrict__ P, const __
         } else if constexpr (MODEL == 1) {
             double2 un = m.bun[b];
             double fv[4];
-            sa_boundary_flux(p.gas, p.pr, p.pr_t, p.t_wall, p.pin, flag, gvx, gvy, E0, dSx, dSy, bdv.x, bdv.y, bLv,
-                             un.x, un.y, m.bds2[b], fv);
+            if (p.sa_cc)
+                sacc_boundary_flux(p.gas, p.pr, p.pr_t, p.t_wall, p.pin, flag, gvx, gvy, E0, dSx, dSy, bdv.x, bdv.y,
+                                   bLv, un.x, un.y, m.bds2[b], fv);
+            else
+                sa_boundary_flux(p.gas, p.pr, p.pr_t, p.t_wall, p.pin, flag, gvx, gvy, E0, dSx, dSy, bdv.x, bdv.y, bLv,
+                                 un.x, un.y, m.bds2[b], fv);
             s.FV[fi] = make_double4(fv[0], fv[1], fv[2], fv[3]);
         } else if (p.laminar == 1) {
             double2 un = m.bun[b];
@@ -716,7 +723,8 @@ __device__ __forceinline__ void gather_residual(const Prm& p, const Mesh& m, con
             double mi_L = sutherland(T);
             double n_L = mi_L / rho;
             double S = fabs(gy.y - gx.z);
-            double Qt = sa_source(n, n_L, S, d, rho, gx.x, gy.x, s.Gxx[c], s.Gxy[c]);
+            double Qt = p.sa_cc ? sacc_source(n, n_L, S, d, rho, gx.x, gy.x, s.Gxx[c], s.Gxy[c])
+                                : sa_source(n, n_L, S, d, rho, gx.x, gy.x, s.Gxx[c], s.Gxy[c]);
             R[4] -= Qt * m.omega[c];
         }
         if constexpr (MODEL == 2) {
