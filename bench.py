@@ -182,7 +182,7 @@ def serve_arm(args):
     import torch
     torch.cuda.set_device(0)
     from csu_b200 import servebench
-    out = servebench.run(n=args.requests, cells_hi=args.cells_hi)
+    out = servebench.run(n=args.requests, cells_hi=args.cells_hi, rate=args.rate)
     b, p = out["batched"], out["plain"]
     line = {"metric": "converged solves/hr", "value": b["solves_per_hour"], "unit": "solves/hr", "n_gpus": 1,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64 residual, f32 DPLUR",
@@ -206,6 +206,7 @@ def main():
                     help="the serving stream instead: batched mixed precision vs plain FP64, one solve at a time")
     ap.add_argument("--requests", type=int, default=40)
     ap.add_argument("--cells-hi", type=float, default=2e5)
+    ap.add_argument("--rate", type=float, default=5.0, help="serving stream: Poisson arrivals per second")
     args = ap.parse_args()
     if args.serve:
         return serve_arm(args)

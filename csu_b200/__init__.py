@@ -131,7 +131,7 @@ class SolveInfo(C.Structure):
 
 class SrvConfig(C.Structure):
     _fields_ = [("budget_bytes", C.c_longlong), ("iters_per_step", C.c_int), ("max_pack", C.c_int),
-                ("rebuild_steps", C.c_int)]
+                ("rebuild_steps", C.c_int), ("prep_threads", C.c_int)]
 
 
 class SrvInfo(C.Structure):
@@ -413,8 +413,8 @@ class Pack:
 class Server:
     """Continuous batching of steady solves (csu_srv_*): submit requests as they arrive, call step() in a loop."""
 
-    def __init__(self, budget_bytes, iters_per_step=16, max_pack=0, rebuild_steps=1):
-        cfg = SrvConfig(int(budget_bytes), int(iters_per_step), int(max_pack), int(rebuild_steps))
+    def __init__(self, budget_bytes, iters_per_step=16, max_pack=0, rebuild_steps=1, prep_threads=0):
+        cfg = SrvConfig(int(budget_bytes), int(iters_per_step), int(max_pack), int(rebuild_steps), int(prep_threads))
         h = C.c_void_p()
         _check(lib().csu_srv_create(C.byref(cfg), C.byref(h)))
         self._h = h

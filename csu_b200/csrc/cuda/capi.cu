@@ -7,6 +7,7 @@
 #include <math.h>
 #include <vector>
 #include <algorithm>
+#include <mutex>
 #include "csu_gpu.h"
 #include "kernels.cuh"
 
@@ -23,6 +24,50 @@ struct Arena {
     char* base = nullptr;
     size_t size = 0, used = 0;
 };
+
+// Device arenas of destroyed packs kept for the next pack: a rebuild makes the new pack before it frees the
+// old one, so two arenas alternate and the serving loop stops allocating and freeing gigabytes per rebuild.
+// An arena is reused when it holds the request and at most twice it; new pack arenas get 25 % headroom.
+std::mutex g_arena_mu;
+std::vector<std::pair<char*, size_t>> g_arena_cache;
+
+cudaError_t pack_arena_take(size_t need, char** base, size_t* size)
+{
+    {
+        std::lock_guard<std::mutex> lk(g_arena_mu);
+        size_t best = g_arena_cache.size();
+        for (size_t k = 0; k < g_arena_cache.size(); k++) {
+            size_t sz = g_arena_cache[k].second;
+            if (sz >= need && sz <= 2 * need && (best == g_arena_cache.size() || sz < g_arena_cache[best].second))
+                best = k;
+        }
+        if (best < g_arena_cache.size()) {
+            *base = g_arena_cache[best].first;
+            *size = g_arena_cache[best].second;
+            g_arena_cache.erase(g_arena_cache.begin() + best);
+            return cudaSuccess;
+        }
+    }
+    size_t want = (need + need / 4 + 255) & ~size_t(255);
+    cudaError_t e = cudaMalloc((void**)base, want);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        want = need;
+        e = cudaMalloc((void**)base, want);
+    }
+    *size = e == cudaSuccess ? want : 0;
+    return e;
+}
+
+void pack_arena_give(char* base, size_t size)
+{
+    std::lock_guard<std::mutex> lk(g_arena_mu);
+    if (g_arena_cache.size() < 2) {
+        g_arena_cache.push_back({base, size});
+        return;
+    }
+    cudaFree(base);
+}
 
 // RK stage coefficients of solverStepRK (solver.c:788-840)
 const double RK1[1] = {1.0};
@@ -519,9 +564,17 @@ static int ctx_setup(csu_ctx* x)
     Arena a;
     plan(x, a);
     size_t bytes = a.size;
-    cudaError_t e = cudaMalloc((void**)&x->arena.base, bytes);
-    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(context arena)");
-    x->arena.size = bytes;
+    cudaError_t e;
+    if (x->is_pack) {
+        size_t got = 0;
+        e = pack_arena_take(bytes, &x->arena.base, &got);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(pack arena)");
+        x->arena.size = got;
+    } else {
+        e = cudaMalloc((void**)&x->arena.base, bytes);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(context arena)");
+        x->arena.size = bytes;
+    }
     x->arena.used = 0;
     plan(x, x->arena);
     e = cudaMemset(x->arena.base, 0, bytes);
@@ -597,6 +650,12 @@ extern "C" int csu_create(const csu_mesh_desc* md, const csu_config* cfg, csu_ct
 extern "C" void csu_destroy(csu_ctx* x)
 {
     if (!x) return;
+    if (x->is_pack && x->arena.base) {
+        // the arena goes back for the next pack to reuse: this pack's work must be done first (while its
+        // streams still exist)
+        if (x->stream) cudaStreamSynchronize(x->stream);
+        if (x->side) cudaStreamSynchronize(x->side);
+    }
     if (x->graph) cudaGraphExecDestroy(x->graph);
     if (x->hist) cudaFree(x->hist);
     for (cudaEvent_t e : x->ev) cudaEventDestroy(e);
@@ -604,9 +663,23 @@ extern "C" void csu_destroy(csu_ctx* x)
     if (x->side) cudaStreamDestroy(x->side);
     if (x->ev_fork) cudaEventDestroy(x->ev_fork);
     if (x->ev_join) cudaEventDestroy(x->ev_join);
-    if (x->arena.base) cudaFree(x->arena.base);
+    if (x->arena.base) {
+        if (x->is_pack) {
+            pack_arena_give(x->arena.base, x->arena.size);
+        } else {
+            cudaFree(x->arena.base);
+        }
+    }
     csu_layout_free(&x->L);
     delete x;
+}
+
+// Frees the pack arenas kept for reuse (the serving layer calls it when it shuts down).
+extern "C" void csu_pack_arena_release(void)
+{
+    std::lock_guard<std::mutex> lk(g_arena_mu);
+    for (auto& a : g_arena_cache) cudaFree(a.first);
+    g_arena_cache.clear();
 }
 
 // State of solve k in its reference order ([var][cell], nvar x its cell count), to or from the device.

@@ -18,14 +18,19 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
+#include <condition_variable>
 #include <deque>
 #include <map>
+#include <mutex>
+#include <thread>
 #include <vector>
 
 #include "csu_gpu.h"
 
 extern "C" void csu_set_error(const char* fmt, ...);
+extern "C" void csu_pack_arena_release(void);
 
 namespace {
 
@@ -39,9 +44,45 @@ struct Group {
     int steps_since = 0;       // steps since the pack was built
 };
 
+// A submitted mesh, owned by the request while a preparation thread builds its layout.
+struct MeshCopy {
+    std::vector<double> xy, wall;
+    std::vector<int> npts, nodes, con, nint, faces, nei, mnbf, mflag, bface;
+    csu_mesh_desc d;
+
+    explicit MeshCopy(const csu_mesh_desc& m) : d(m)
+    {
+        const size_t nc = (size_t)m.n_cells, nf = (size_t)m.n_faces, nb = (size_t)m.n_bfaces;
+        xy.assign(m.xy, m.xy + 2 * (size_t)m.n_points);
+        npts.assign(m.cell_npts, m.cell_npts + nc);
+        nodes.assign(m.cell_nodes, m.cell_nodes + 4 * nc);
+        con.assign(m.con, m.con + 4 * nf);
+        nint.assign(m.cell_nint, m.cell_nint + nc);
+        faces.assign(m.cell_faces, m.cell_faces + 4 * nc);
+        nei.assign(m.cell_nei, m.cell_nei + 4 * nc);
+        mnbf.assign(m.marker_nbf, m.marker_nbf + m.n_markers);
+        mflag.assign(m.marker_flag, m.marker_flag + m.n_markers);
+        bface.assign(m.bface, m.bface + 3 * nb);
+        if (m.wall_dist) wall.assign(m.wall_dist, m.wall_dist + nc);
+        d.xy = xy.data();
+        d.cell_npts = npts.data();
+        d.cell_nodes = nodes.data();
+        d.con = con.data();
+        d.cell_nint = nint.data();
+        d.cell_faces = faces.data();
+        d.cell_nei = nei.data();
+        d.marker_nbf = mnbf.data();
+        d.marker_flag = mflag.data();
+        d.bface = bface.data();
+        d.wall_dist = m.wall_dist ? wall.data() : nullptr;
+    }
+};
+
 struct Req {
     long long id = 0;
     csu_prep* prep = nullptr;
+    MeshCopy* mesh = nullptr;  // while a preparation thread has it
+    std::atomic<int> ready{1}; // 0 being prepared, 1 prepared, 2 preparation failed
     csu_config cfg;
     std::vector<double> U;     // initial state, then the final one
     int nv = 0, nc = 0;
@@ -80,6 +121,12 @@ struct csu_srv {
     double t_rebuild = 0, t_iterate = 0, t_poll = 0; // host seconds in the phases of csu_srv_step
     int rebuilds = 0;
     std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+    // preparation threads (prep_threads > 0)
+    std::vector<std::thread> workers;
+    std::mutex mu;
+    std::condition_variable cv;
+    std::deque<Req*> todo;
+    bool stop = false;
 
     double now() const
     {
@@ -100,12 +147,68 @@ extern "C" int csu_srv_create(const csu_srv_config* cfg, csu_srv** out)
     return CSU_OK;
 }
 
+// Builds a request's layout on a preparation thread; the step loop admits it once `ready` says so.
+static void prepare(csu_srv* s, Req* r)
+{
+    csu_prep* p = nullptr;
+    int st = csu_prep_create(&r->mesh->d, &r->cfg, &p);
+    if (!st && csu_prep_bytes(p) > s->cfg.budget_bytes) {
+        csu_prep_destroy(p);
+        p = nullptr;
+        st = CSU_ERR_OOM;
+    }
+    delete r->mesh;
+    r->mesh = nullptr;
+    r->prep = p;
+    r->bytes = p ? csu_prep_bytes(p) : 0;
+    r->ready.store(st ? 2 : 1, std::memory_order_release);
+}
+
+static void prep_worker(csu_srv* s)
+{
+    for (;;) {
+        Req* r;
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            s->cv.wait(lk, [s] { return s->stop || !s->todo.empty(); });
+            if (s->stop) return;
+            r = s->todo.front();
+            s->todo.pop_front();
+        }
+        prepare(s, r);
+    }
+}
+
 extern "C" int csu_srv_submit(csu_srv* s, const csu_mesh_desc* mesh, const csu_config* cfg, const double* U0,
                               int max_iters, long long* id)
 {
     if (!s || !mesh || !cfg || !U0 || max_iters < 1) return CSU_ERR_INPUT;
     csu_config c = *cfg;
     c.iter_cap = max_iters; // the pack freezes the solve at its cap, whatever the step length
+    if (s->cfg.prep_threads > 0) {
+        if (mesh->n_cells <= 0) return CSU_ERR_INPUT;
+        Req* r = new Req();
+        r->id = s->next_id++;
+        r->cfg = c;
+        r->nv = cfg->nvar;
+        r->nc = mesh->n_cells;
+        r->U.assign(U0, U0 + (size_t)r->nv * r->nc);
+        r->max_iters = max_iters;
+        r->t_submit = s->now();
+        r->mesh = new MeshCopy(*mesh);
+        r->ready.store(0, std::memory_order_relaxed);
+        s->reqs[r->id] = r;
+        s->queue.push_back(r);
+        if (s->workers.empty())
+            for (int k = 0; k < s->cfg.prep_threads; k++) s->workers.emplace_back(prep_worker, s);
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->todo.push_back(r);
+        }
+        s->cv.notify_one();
+        if (id) *id = r->id;
+        return CSU_OK;
+    }
     csu_prep* p = nullptr;
     int st = csu_prep_create(mesh, &c, &p);
     if (st) return st;
@@ -231,6 +334,17 @@ extern "C" int csu_srv_step(csu_srv* s, int* n_running, int* n_queued)
     const int every = s->cfg.rebuild_steps > 1 ? s->cfg.rebuild_steps : 1;
     for (auto it = s->queue.begin(); it != s->queue.end();) {
         Req* r = *it;
+        const int rd = r->ready.load(std::memory_order_acquire);
+        if (rd == 0) { // still being prepared
+            ++it;
+            continue;
+        }
+        if (rd == 2) { // its layout failed or it exceeds the budget
+            r->state = CSU_SRV_FAILED;
+            r->t_start = r->t_end = s->now();
+            it = s->queue.erase(it);
+            continue;
+        }
         Group* g = group_for(s, r->cfg);
         bool window = !g->pack || active(g) == 0 || g->steps_since >= every;
         int size = active(g) + (int)g->pending.size();
@@ -333,6 +447,13 @@ extern "C" int csu_srv_totals(csu_srv* s, long long* solve_iterations, long long
 extern "C" void csu_srv_destroy(csu_srv* s)
 {
     if (!s) return;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->todo.clear();
+        s->stop = true;
+    }
+    s->cv.notify_all();
+    for (std::thread& t : s->workers) t.join();
     for (Group* g : s->groups) {
         for (Req* r : g->members)
             if (r->taken) {
@@ -344,7 +465,9 @@ extern "C" void csu_srv_destroy(csu_srv* s)
     }
     for (auto& kv : s->reqs) {
         if (kv.second->prep) csu_prep_destroy(kv.second->prep);
+        delete kv.second->mesh;
         delete kv.second;
     }
+    csu_pack_arena_release();
     delete s;
 }

@@ -90,8 +90,10 @@ def run_plain(reqs, cases, max_iters):
     return res, states, cu, time.perf_counter() - t0
 
 
-def run_batched(reqs, cases, max_iters, budget_bytes, iters_per_step=16, rebuild_steps=8):
-    srv = Server(budget_bytes, iters_per_step=iters_per_step, rebuild_steps=rebuild_steps)
+def run_batched(reqs, cases, max_iters, budget_bytes, iters_per_step=16, rebuild_steps=8, prep_threads=2):
+    # meshes are prepared on background threads while the packs iterate
+    srv = Server(budget_bytes, iters_per_step=iters_per_step, rebuild_steps=rebuild_steps,
+                 prep_threads=prep_threads)
     t0 = time.perf_counter()
     ids = [None] * len(reqs)
     nxt = 0

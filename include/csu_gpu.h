@@ -296,6 +296,11 @@ typedef struct csu_srv_config {
     int rebuild_steps;       /* admit into a running pack at most every this many steps (a pack
                                 rebuild re-uploads its meshes; finished solves stay frozen in the
                                 pack until the next rebuild); 0 or 1: every step                  */
+    int prep_threads;        /* host threads that build submitted meshes' device layouts while the
+                                packs iterate (csu_srv_submit then copies the mesh and returns at
+                                once; a request is admitted once prepared, and one whose layout
+                                fails or exceeds the budget ends CSU_SRV_FAILED); 0: csu_srv_submit
+                                prepares the mesh itself and reports those errors                  */
 } csu_srv_config;
 typedef struct csu_srv_request_info {
     int state;               /* CSU_SRV_*                                                      */

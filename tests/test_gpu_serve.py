@@ -34,10 +34,11 @@ def _alone(name, kv):
     return len(h), U
 
 
-@pytest.mark.parametrize("budget_mb", [4096, 18])
-def test_served_results_equal_alone(native, budget_mb):
+@pytest.mark.parametrize("budget_mb,prep_threads", [(4096, 0), (18, 0), (4096, 2), (18, 2)])
+def test_served_results_equal_alone(native, budget_mb, prep_threads):
+    """prep_threads 2: the meshes are prepared on background threads while the packs iterate"""
     import csu_b200
-    srv = csu_b200.Server(budget_mb << 20, iters_per_step=16)
+    srv = csu_b200.Server(budget_mb << 20, iters_per_step=16, prep_threads=prep_threads)
     ids = []
     for k, (nm, kv) in enumerate(REQUESTS):
         ids.append(srv.submit(_case(nm, kv), max_iters=MAX_IT))
