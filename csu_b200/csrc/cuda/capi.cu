@@ -674,12 +674,17 @@ extern "C" void csu_destroy(csu_ctx* x)
     delete x;
 }
 
+static void release_copy_jobs();
+
 // Frees the pack arenas kept for reuse (the serving layer calls it when it shuts down).
 extern "C" void csu_pack_arena_release(void)
 {
-    std::lock_guard<std::mutex> lk(g_arena_mu);
-    for (auto& a : g_arena_cache) cudaFree(a.first);
-    g_arena_cache.clear();
+    {
+        std::lock_guard<std::mutex> lk(g_arena_mu);
+        for (auto& a : g_arena_cache) cudaFree(a.first);
+        g_arena_cache.clear();
+    }
+    release_copy_jobs();
 }
 
 // State of solve k in its reference order ([var][cell], nvar x its cell count), to or from the device.
@@ -1515,6 +1520,9 @@ extern "C" int csu_pack_history(csu_ctx* x, int k, double* hist, int max_rows, i
 // Device copy of solve kf of `from` into solve kt of `to` (same mesh and settings): conserved state,
 // primitives, the implicit increments (DPLUR warm start) and the solve's counters, first residual and
 // flags, so that `to` continues the solve where `from` left it.
+struct CopyPlan;
+static void state_copy_plan(csu_ctx* from, int kf, csu_ctx* to, int kt, CopyPlan& plan);
+
 extern "C" int csu_pack_transfer(csu_ctx* from, int kf, csu_ctx* to, int kt)
 {
     if (!from || !to || kf < 0 || kf >= from->nsolve || kt < 0 || kt >= to->nsolve) return CSU_ERR_INPUT;
@@ -1697,8 +1705,110 @@ static SegGeo seg_geo(const csu_ctx* x, int k)
     return g;
 }
 
-// Copies solve k's mesh rows into x: device to device from solve ks of `src`, or from `L` (src null).
-static int seg_fill(csu_ctx* x, int k, const csu_layout* L, csu_ctx* src, int ks)
+// Device-to-device copies of a pack rebuild, gathered into one table and run by one kernel (a rebuild of a
+// large pack would otherwise issue thousands of small copies). Jobs are split into pieces of at most 256 KiB
+// so the blocks share the work; each piece moves 8-byte words when its addresses and length allow.
+struct CopyJob {
+    const char* src;
+    char* dst;
+    unsigned long long bytes;
+};
+
+struct CopyPlan {
+    std::vector<CopyJob> jobs;
+    void add(void* dst, const void* src, size_t bytes)
+    {
+        const size_t piece = 256 << 10;
+        for (size_t o = 0; o < bytes; o += piece)
+            jobs.push_back({(const char*)src + o, (char*)dst + o, (unsigned long long)std::min(piece, bytes - o)});
+    }
+};
+
+__global__ void k_copy_jobs(const CopyJob* __restrict__ jobs, int n)
+{
+    for (int j = blockIdx.x; j < n; j += gridDim.x) {
+        const CopyJob J = jobs[j];
+        if ((((unsigned long long)J.src | (unsigned long long)J.dst | J.bytes) & 7) == 0) {
+            const unsigned long long* s = reinterpret_cast<const unsigned long long*>(J.src);
+            unsigned long long* d = reinterpret_cast<unsigned long long*>(J.dst);
+            for (unsigned long long i = threadIdx.x; i < J.bytes / 8; i += blockDim.x) d[i] = s[i];
+        } else {
+            for (unsigned long long i = threadIdx.x; i < J.bytes; i += blockDim.x) J.dst[i] = J.src[i];
+        }
+    }
+}
+
+// the device copy of a plan's job table, kept and grown across rebuilds (freed with the pack arenas)
+std::mutex g_jobs_mu;
+CopyJob* g_jobs_dev = nullptr;
+size_t g_jobs_cap = 0;
+
+static int run_copy_plan(csu_ctx* x, CopyPlan& plan)
+{
+    if (plan.jobs.empty()) return CSU_OK;
+    std::lock_guard<std::mutex> lk(g_jobs_mu);
+    const size_t n = plan.jobs.size();
+    if (n > g_jobs_cap) {
+        if (g_jobs_dev) cudaFree(g_jobs_dev);
+        g_jobs_dev = nullptr;
+        g_jobs_cap = 0;
+        size_t cap = std::max(n, (size_t)4096);
+        CK(cudaMalloc((void**)&g_jobs_dev, sizeof(CopyJob) * cap));
+        g_jobs_cap = cap;
+    }
+    CK(cudaMemcpyAsync(g_jobs_dev, plan.jobs.data(), sizeof(CopyJob) * n, cudaMemcpyHostToDevice, x->stream));
+    k_copy_jobs<<<(int)std::min(n, (size_t)(148 * 8)), 256, 0, x->stream>>>(g_jobs_dev, (int)n);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(x->stream)); // the table is reused by the next plan
+    plan.jobs.clear();
+    return CSU_OK;
+}
+
+// The iteration state of solve kf of `from` (U, W, T, Omega/Lc or local steps, both DPLUR increments) queued
+// as copies into solve kt of `to`; the scalars are the caller's (csu_pack_transfer moves the same arrays).
+static void state_copy_plan(csu_ctx* from, int kf, csu_ctx* to, int kt, CopyPlan& plan)
+{
+    const int n = from->ncs[kf], of = from->cell0[kf], ot = to->cell0[kt], NF = from->L.nc, NT = to->L.nc;
+    const int nx = from->nv - 4;
+    plan.add(to->st.U4 + ot, from->st.U4 + of, sizeof(double4) * n);
+    plan.add(to->st.W4 + ot, from->st.W4 + of, sizeof(double4) * n);
+    plan.add(to->st.WT + ot, from->st.WT + of, sizeof(double) * n);
+    plan.add(to->st.dtl + ot, from->st.dtl + of, sizeof(double) * n);
+    for (int r = 0; r < nx; r++) {
+        plan.add(to->st.Ux + (size_t)r * NT + ot, from->st.Ux + (size_t)r * NF + of, sizeof(double) * n);
+        plan.add(to->st.Wx + (size_t)r * NT + ot, from->st.Wx + (size_t)r * NF + of, sizeof(double) * n);
+    }
+    if (from->st.X4[0] && to->st.X4[0]) {
+        for (int q = 0; q < 2; q++) {
+            int qf = from->xcur ^ q, qt = to->xcur ^ q;
+            plan.add(to->st.X4[qt] + ot, from->st.X4[qf] + of, sizeof(double4) * n);
+            for (int r = 0; r < nx; r++)
+                plan.add(to->st.Xx[qt] + (size_t)r * NT + ot, from->st.Xx[qf] + (size_t)r * NF + of,
+                         sizeof(double) * n);
+        }
+    }
+}
+
+static void release_copy_jobs()
+{
+    std::lock_guard<std::mutex> lk(g_jobs_mu);
+    if (g_jobs_dev) cudaFree(g_jobs_dev);
+    g_jobs_dev = nullptr;
+    g_jobs_cap = 0;
+}
+
+// Re-bases the index-valued rows of one solve whose rows are in place (k_seg_fix).
+static int seg_fix(csu_ctx* x, SegGeo S, SegGeo D)
+{
+    int nt = std::max(D.nc, std::max(D.nf, D.nb));
+    if (nt > 0) k_seg_fix<<<(nt + BLOCK - 1) / BLOCK, BLOCK, 0, x->stream>>>(x->mesh, x->d_wall_rank, S, D);
+    CK(cudaGetLastError());
+    return CSU_OK;
+}
+
+// Copies solve k's mesh rows into x: device to device from solve ks of `src` (queued on `plan`, and
+// re-based by k_seg_fix once the plan has run: see seg_fix), or from `L` (src null).
+static int seg_fill(csu_ctx* x, int k, const csu_layout* L, csu_ctx* src, int ks, CopyPlan* plan)
 {
     SegGeo D = seg_geo(x, k), S;
     std::vector<SegArr> dst = seg_arrays(x);
@@ -1709,8 +1819,8 @@ static int seg_fill(csu_ctx* x, int k, const csu_layout* L, csu_ctx* src, int ks
         for (size_t a = 0; a < dst.size(); a++) {
             const size_t es = dst[a].es;
             auto cp = [&](size_t so, size_t dof, size_t n) {
-                return cudaMemcpyAsync(dst[a].dev + dof * es, from[a].dev + so * es, n * es,
-                                       cudaMemcpyDeviceToDevice, x->stream);
+                plan->add(dst[a].dev + dof * es, from[a].dev + so * es, n * es);
+                return cudaSuccess;
             };
             switch (dst[a].kind) {
             case SEG_CELL: CK(cp(S.c0, D.c0, D.nc)); break;
@@ -1743,9 +1853,7 @@ static int seg_fill(csu_ctx* x, int k, const csu_layout* L, csu_ctx* src, int ks
             }
         }
     }
-    int nt = std::max(D.nc, std::max(D.nf, D.nb));
-    if (nt > 0) k_seg_fix<<<(nt + BLOCK - 1) / BLOCK, BLOCK, 0, x->stream>>>(x->mesh, x->d_wall_rank, S, D);
-    CK(cudaGetLastError());
+    if (!src) return seg_fix(x, S, D);
     return CSU_OK;
 }
 
@@ -1836,11 +1944,20 @@ static int pack_build(const char* who, const csu_prep* const* solves, int n, csu
             for (int c = 0; c < solves[k]->L.nc; c++) color_cells[fill[solves[k]->L.color[c]]++] = x->cell0[k] + c;
     }
     int st = ctx_setup(x);
-    // mesh rows, solve maps and colour lists
+    // mesh rows (kept solves: one batched device copy, then their re-basing), solve maps and colour lists
+    CopyPlan plan;
+    if (!st && old) {
+        // the old pack's last iterations must be done before its rows are read from another stream
+        cudaError_t e = cudaStreamSynchronize(old->stream);
+        if (e != cudaSuccess) st = cuda_fail(e, "pack rebuild");
+    }
     for (int k = 0; k < n && !st; k++) {
         bool kept = old && keep && keep[k] >= 0;
-        st = kept ? seg_fill(x, k, nullptr, old, keep[k]) : seg_fill(x, k, &solves[k]->L, nullptr, 0);
+        st = kept ? seg_fill(x, k, nullptr, old, keep[k], &plan) : seg_fill(x, k, &solves[k]->L, nullptr, 0, &plan);
     }
+    if (!st) st = run_copy_plan(x, plan);
+    for (int k = 0; k < n && !st; k++)
+        if (old && keep && keep[k] >= 0) st = seg_fix(x, seg_geo(old, keep[k]), seg_geo(x, k));
     if (!st) {
         int nblk = (NC + BLOCK - 1) / BLOCK;
         std::vector<int> bs(nblk, 0), cs(NC, 0);
@@ -1857,9 +1974,26 @@ static int pack_build(const char* who, const csu_prep* const* solves, int n, csu
                            cudaMemcpyHostToDevice);
         if (e != cudaSuccess) st = cuda_fail(e, "pack maps");
     }
-    // iteration state of the kept solves
-    for (int k = 0; k < n && !st; k++)
-        if (old && keep && keep[k] >= 0) st = csu_pack_transfer(old, keep[k], x, k);
+    // iteration state of the kept solves: one batched copy, their scalars in one read and one write
+    if (!st && old && keep) {
+        std::vector<Scalars> ho(old->nsolve), hn(n);
+        st = read_scalars_n(old, ho.data(), old->nsolve);
+        if (!st) st = read_scalars_n(x, hn.data(), n);
+        for (int k = 0; k < n && !st; k++) {
+            if (keep[k] < 0) continue;
+            state_copy_plan(old, keep[k], x, k, plan);
+            Scalars h = ho[keep[k]];
+            h.hist = hn[k].hist;
+            h.hist_cap = hn[k].hist_cap;
+            h.hist_row = 0;
+            h.steps = 0;
+            h.fresh = 0;
+            hn[k] = h;
+        }
+        if (!st) st = run_copy_plan(x, plan);
+        if (!st) st = write_scalars_n(x, hn.data(), n);
+        x->prepared = 0;
+    }
     if (st) {
         csu_destroy(x);
         return st;
