@@ -1520,8 +1520,7 @@ extern "C" int csu_pack_history(csu_ctx* x, int k, double* hist, int max_rows, i
 // Device copy of solve kf of `from` into solve kt of `to` (same mesh and settings): conserved state,
 // primitives, the implicit increments (DPLUR warm start) and the solve's counters, first residual and
 // flags, so that `to` continues the solve where `from` left it.
-struct CopyPlan;
-static void state_copy_plan(csu_ctx* from, int kf, csu_ctx* to, int kt, CopyPlan& plan);
+static int transfer_state_copies(csu_ctx* from, int kf, csu_ctx* to, int kt);
 
 extern "C" int csu_pack_transfer(csu_ctx* from, int kf, csu_ctx* to, int kt)
 {
@@ -1530,27 +1529,10 @@ extern "C" int csu_pack_transfer(csu_ctx* from, int kf, csu_ctx* to, int kt)
         csu_set_error("csu_pack_transfer: the two solves differ in size or settings");
         return CSU_ERR_INPUT;
     }
-    const int n = from->ncs[kf], of = from->cell0[kf], ot = to->cell0[kt], NF = from->L.nc, NT = to->L.nc;
-    const int nx = from->nv - 4;
     CK(cudaStreamSynchronize(from->stream));
     CK(cudaStreamSynchronize(to->stream));
-    auto cp = [&](void* dst, const void* src, size_t bytes) { return cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToDevice); };
-    CK(cp(to->st.U4 + ot, from->st.U4 + of, sizeof(double4) * n));
-    CK(cp(to->st.W4 + ot, from->st.W4 + of, sizeof(double4) * n));
-    CK(cp(to->st.WT + ot, from->st.WT + of, sizeof(double) * n));
-    CK(cp(to->st.dtl + ot, from->st.dtl + of, sizeof(double) * n));
-    for (int r = 0; r < nx; r++) {
-        CK(cp(to->st.Ux + (size_t)r * NT + ot, from->st.Ux + (size_t)r * NF + of, sizeof(double) * n));
-        CK(cp(to->st.Wx + (size_t)r * NT + ot, from->st.Wx + (size_t)r * NF + of, sizeof(double) * n));
-    }
-    if (from->st.X4[0] && to->st.X4[0]) {
-        for (int q = 0; q < 2; q++) {
-            int qf = from->xcur ^ q, qt = to->xcur ^ q;
-            CK(cp(to->st.X4[qt] + ot, from->st.X4[qf] + of, sizeof(double4) * n));
-            for (int r = 0; r < nx; r++)
-                CK(cp(to->st.Xx[qt] + (size_t)r * NT + ot, from->st.Xx[qf] + (size_t)r * NF + of, sizeof(double) * n));
-        }
-    }
+    int st = transfer_state_copies(from, kf, to, kt);
+    if (st) return st;
     Scalars hf, ht;
     CK(cudaMemcpy(&hf, from->st.sc + kf, sizeof(Scalars), cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(&ht, to->st.sc + kt, sizeof(Scalars), cudaMemcpyDeviceToHost));
@@ -1795,6 +1777,14 @@ static void release_copy_jobs()
     if (g_jobs_dev) cudaFree(g_jobs_dev);
     g_jobs_dev = nullptr;
     g_jobs_cap = 0;
+}
+
+// The state copies of csu_pack_transfer, run at once.
+static int transfer_state_copies(csu_ctx* from, int kf, csu_ctx* to, int kt)
+{
+    CopyPlan plan;
+    state_copy_plan(from, kf, to, kt, plan);
+    return run_copy_plan(to, plan);
 }
 
 // Re-bases the index-valued rows of one solve whose rows are in place (k_seg_fix).
