@@ -20,6 +20,22 @@ def test_ext80_matches_x87(tmp_path):
 
 
 @pytest.mark.skipif(platform.machine() != "x86_64", reason="needs x87 long double")
+def test_x87_quotient_of_doubles(tmp_path):
+    """lsqdd.cuh x87_div_d, the SST LU-SGS diagonal's `long double` quotient stored to double, equals the
+    host's x87 on random, exact and near-midpoint quotients -- where a plain double division differs
+    (double rounding) in a few hundred cases."""
+    exe = str(tmp_path / "x87div_check")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-ffp-contract=off", "-o", exe,
+                    os.path.join(ROOT, "tests", "native", "x87div_check.cpp")], check=True)
+    r = subprocess.run([exe, "200000"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    f = dict(kv.split("=") for kv in r.stdout.split() if "=" in kv)
+    assert f["mismatches"] == "0", r.stdout
+    assert int(f["naive_differs"]) > 0, r.stdout  # the cases exercise the double rounding
+    assert int(f["decided"]) > 0.999 * int(f["tried"]), r.stdout
+
+
+@pytest.mark.skipif(platform.machine() != "x86_64", reason="needs x87 long double")
 def test_certified_double_double_matches_x87(tmp_path):
     """lsqdd.cuh: the FP64 emulation of single x87 operations (accumulation step, product, sum) equals the
     host's x87 results on random, tie-prone, power-of-two and cancelling operands, and every gradient
