@@ -139,6 +139,21 @@ def alg_bytes(case):
     }
 
 
+def max_over_ranks(ms, dist, device):
+    """The job's time: the slowest rank's. Every rank takes part in the same all-reduce (no-op alone)."""
+    if not dist:
+        return ms
+    import torch
+    t = torch.tensor([ms], device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(cells, steps, world, ms):
+    """Cell-updates per second of the whole job: every replica advances its own mesh `steps` times."""
+    return cells * steps * world / (ms / 1e3)
+
+
 def run_reference(wd, steps, warmup):
     """The reference's own solver functions (oracle/_ref), OpenMP on all host cores."""
     from oracle.refharness import Ref, available
@@ -249,13 +264,10 @@ def main():
         torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
     launches = eng.stats()["kernel_launches"] - launches0
+    ms = max_over_ranks(ms, dist, "cuda")
     if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        if dist:
-            dist.barrier()
-    value = nc * args.steps * world / (ms / 1e3)
+        dist.barrier()
+    value = job_throughput(nc, args.steps, world, ms)
 
     # per-kernel device times of a few iterations, for the roofline of the dominant kernel
     kt = eng.time_kernels(5)
