@@ -38,7 +38,7 @@ def test_replicas_report_the_slowest_rank():
     sys.path.insert(0, ROOT)
     import bench
     world = 2
-    with mp.Manager() as mgr:
+    with mp.get_context("spawn").Manager() as mgr:
         out = mgr.dict()
         mp.spawn(_rank, args=(world, _free_port(), out), nprocs=world, join=True)
         got = dict(out)
