@@ -116,6 +116,9 @@ def lib():
         L.csu_srv_step.argtypes = [vp, ip, ip]
         L.csu_srv_info.argtypes = [vp, C.c_longlong, C.POINTER(SrvInfo)]
         L.csu_srv_take.argtypes = [vp, C.c_longlong, vp]
+        L.csu_srv_cancel.argtypes = [vp, C.c_longlong]
+        L.csu_srv_message.argtypes = [vp, C.c_longlong, C.c_char_p, C.c_int]
+        L.csu_pack_stop.argtypes = [vp, C.c_int]
         L.csu_srv_totals.argtypes = [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
         L.csu_srv_times.argtypes = [vp, dp, dp, dp, ip]
         L.csu_srv_destroy.argtypes = [vp]
@@ -136,10 +139,10 @@ class SrvConfig(C.Structure):
 
 class SrvInfo(C.Structure):
     _fields_ = [("state", C.c_int), ("iters", C.c_int), ("n_cells", C.c_int), ("drop", C.c_double),
-                ("t_submit", C.c_double), ("t_start", C.c_double), ("t_end", C.c_double)]
+                ("t_submit", C.c_double), ("t_start", C.c_double), ("t_end", C.c_double), ("status", C.c_int)]
 
 
-SRV_STATES = {0: "queued", 1: "running", 2: "converged", 3: "failed", 4: "maxiter"}
+SRV_STATES = {0: "queued", 1: "running", 2: "converged", 3: "failed", 4: "maxiter", 5: "cancelled"}
 
 
 def _check(st):
@@ -393,6 +396,10 @@ class Pack:
                 new.set_state(k, p.state)
         return new
 
+    def stop(self, k):
+        """Freezes solve k where it stands; the others go on."""
+        _check(lib().csu_pack_stop(self._h, k))
+
     def transfer_from(self, other, k_other, k):
         _check(lib().csu_pack_transfer(other._h, k_other, self._h, k))
 
@@ -438,7 +445,15 @@ class Server:
         i = SrvInfo()
         _check(lib().csu_srv_info(self._h, rid, C.byref(i)))
         return {"state": SRV_STATES[i.state], "iters": i.iters, "n_cells": i.n_cells, "drop": i.drop,
-                "t_submit": i.t_submit, "t_start": i.t_start, "t_end": i.t_end}
+                "t_submit": i.t_submit, "t_start": i.t_start, "t_end": i.t_end, "status": i.status}
+
+    def cancel(self, rid):
+        _check(lib().csu_srv_cancel(self._h, rid))
+
+    def message(self, rid):
+        buf = C.create_string_buffer(256)
+        _check(lib().csu_srv_message(self._h, rid, buf, 256))
+        return buf.value.decode(errors="replace")
 
     def take(self, rid):
         U = np.zeros(self._shape[rid])

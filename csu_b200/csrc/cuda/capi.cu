@@ -28,22 +28,29 @@ struct Arena {
 // Device arenas of destroyed packs kept for the next pack: a rebuild makes the new pack before it frees the
 // old one, so two arenas alternate and the serving loop stops allocating and freeing gigabytes per rebuild.
 // An arena is reused when it holds the request and at most twice it; new pack arenas get 25 % headroom.
+// Entries remember their device: a pack takes only arenas of the device current when it is made.
+struct CachedArena {
+    int dev;
+    char* base;
+    size_t size;
+};
 std::mutex g_arena_mu;
-std::vector<std::pair<char*, size_t>> g_arena_cache;
+std::vector<CachedArena> g_arena_cache;
 
-cudaError_t pack_arena_take(size_t need, char** base, size_t* size)
+cudaError_t pack_arena_take(int dev, size_t need, char** base, size_t* size)
 {
     {
         std::lock_guard<std::mutex> lk(g_arena_mu);
         size_t best = g_arena_cache.size();
         for (size_t k = 0; k < g_arena_cache.size(); k++) {
-            size_t sz = g_arena_cache[k].second;
-            if (sz >= need && sz <= 2 * need && (best == g_arena_cache.size() || sz < g_arena_cache[best].second))
+            if (g_arena_cache[k].dev != dev) continue;
+            size_t sz = g_arena_cache[k].size;
+            if (sz >= need && sz <= 2 * need && (best == g_arena_cache.size() || sz < g_arena_cache[best].size))
                 best = k;
         }
         if (best < g_arena_cache.size()) {
-            *base = g_arena_cache[best].first;
-            *size = g_arena_cache[best].second;
+            *base = g_arena_cache[best].base;
+            *size = g_arena_cache[best].size;
             g_arena_cache.erase(g_arena_cache.begin() + best);
             return cudaSuccess;
         }
@@ -59,11 +66,13 @@ cudaError_t pack_arena_take(size_t need, char** base, size_t* size)
     return e;
 }
 
-void pack_arena_give(char* base, size_t size)
+void pack_arena_give(int dev, char* base, size_t size)
 {
     std::lock_guard<std::mutex> lk(g_arena_mu);
-    if (g_arena_cache.size() < 2) {
-        g_arena_cache.push_back({base, size});
+    int held = 0;
+    for (const CachedArena& a : g_arena_cache) held += a.dev == dev;
+    if (held < 2) {
+        g_arena_cache.push_back({dev, base, size});
         return;
     }
     cudaFree(base);
@@ -112,15 +121,20 @@ struct csu_ctx {
     int hist_cap = 0;
     int gb_c = 0;
     const double* rk = nullptr;
-    cudaGraphExec_t graph = nullptr;
-    int graph_iters = 0;
-    long long graph_launches = 0;
+    // CUDA graphs of GRAPH_SIZES[g] iterations, one per DPLUR increment-buffer parity at their start (an odd
+    // Nlinear flips it every iteration); captured on first use, kept until the launch sequence changes
+    cudaGraphExec_t graphs[4][2] = {};
+    long long graph_launches[4][2] = {};
+    Scalars* h_sc = nullptr;   // pinned: solve 0's scalars, read back once at the end of csu_iterate
+    double* h_hist = nullptr;  // pinned: solve 0's history rows (hist_cap rows)
     int have_debug = 0;
     cudaStream_t own_stream = nullptr;
     // DPLUR blocks run on a side stream, forked from and joined back to the engine stream
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int max_ni = 4;          // most interior faces of a cell (k_blocks covers slots [0, max_ni))
+    int device = 0;          // the CUDA device current when the context was made (its memory lives there)
+    int sm_count = 148;      // that device's multiprocessors
     // one-solve contexts: the renumbering on the device and a staging buffer for the state in reference order
     int* d_n2o = nullptr;
     double* d_stage = nullptr;
@@ -146,6 +160,19 @@ static void tmark(csu_ctx* x, int kind)
     x->ev_kind[x->ev_used] = kind;
     cudaEventRecord(x->ev[x->ev_used], x->stream);
     x->ev_used++;
+}
+
+// iterations per captured graph; a call of n iterations replays the largest first (n = 8a + 4b + 2c + d)
+static const int GRAPH_SIZES[4] = {8, 4, 2, 1};
+
+static void drop_graphs(csu_ctx* x)
+{
+    for (int g = 0; g < 4; g++)
+        for (int q = 0; q < 2; q++) {
+            if (x->graphs[g][q]) cudaGraphExecDestroy(x->graphs[g][q]);
+            x->graphs[g][q] = nullptr;
+            x->graph_launches[g][q] = 0;
+        }
 }
 
 static int cuda_fail(cudaError_t e, const char* what)
@@ -565,9 +592,12 @@ static int ctx_setup(csu_ctx* x)
     plan(x, a);
     size_t bytes = a.size;
     cudaError_t e;
+    e = cudaGetDevice(&x->device);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&x->sm_count, cudaDevAttrMultiProcessorCount, x->device);
+    if (e != cudaSuccess) return cuda_fail(e, "device query");
     if (x->is_pack) {
         size_t got = 0;
-        e = pack_arena_take(bytes, &x->arena.base, &got);
+        e = pack_arena_take(x->device, bytes, &x->arena.base, &got);
         if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(pack arena)");
         x->arena.size = got;
     } else {
@@ -656,8 +686,10 @@ extern "C" void csu_destroy(csu_ctx* x)
         if (x->stream) cudaStreamSynchronize(x->stream);
         if (x->side) cudaStreamSynchronize(x->side);
     }
-    if (x->graph) cudaGraphExecDestroy(x->graph);
+    drop_graphs(x);
     if (x->hist) cudaFree(x->hist);
+    if (x->h_sc) cudaFreeHost(x->h_sc);
+    if (x->h_hist) cudaFreeHost(x->h_hist);
     for (cudaEvent_t e : x->ev) cudaEventDestroy(e);
     if (x->own_stream) cudaStreamDestroy(x->own_stream);
     if (x->side) cudaStreamDestroy(x->side);
@@ -665,7 +697,7 @@ extern "C" void csu_destroy(csu_ctx* x)
     if (x->ev_join) cudaEventDestroy(x->ev_join);
     if (x->arena.base) {
         if (x->is_pack) {
-            pack_arena_give(x->arena.base, x->arena.size);
+            pack_arena_give(x->device, x->arena.base, x->arena.size);
         } else {
             cudaFree(x->arena.base);
         }
@@ -681,7 +713,7 @@ extern "C" void csu_pack_arena_release(void)
 {
     {
         std::lock_guard<std::mutex> lk(g_arena_mu);
-        for (auto& a : g_arena_cache) cudaFree(a.first);
+        for (const CachedArena& a : g_arena_cache) cudaFree(a.base);
         g_arena_cache.clear();
     }
     release_copy_jobs();
@@ -1013,8 +1045,13 @@ static int ensure_hist(csu_ctx* x, int n)
     if (x->hist) CK(cudaFree(x->hist));
     x->hist = nullptr;
     CK(cudaMalloc((void**)&x->hist, sizeof(double) * (size_t)cap * (x->nv + 4) * x->nsolve));
+    if (!x->is_pack) {
+        if (x->h_hist) CK(cudaFreeHost(x->h_hist));
+        x->h_hist = nullptr;
+        CK(cudaMallocHost((void**)&x->h_hist, sizeof(double) * (size_t)cap * (x->nv + 4)));
+    }
     x->hist_cap = cap;
-    // point every solve's scalars at its new rows
+    // point every solve's scalars at its new rows (the graphs read the pointer from the scalars at run time)
     std::vector<Scalars> hs(x->nsolve);
     int st;
     if ((st = read_scalars_n(x, hs.data(), x->nsolve))) return st;
@@ -1022,76 +1059,99 @@ static int ensure_hist(csu_ctx* x, int n)
         hs[k].hist = hist_of(x, k);
         hs[k].hist_cap = cap;
     }
-    if ((st = write_scalars_n(x, hs.data(), x->nsolve))) return st;
-    if (x->graph) {
-        cudaGraphExecDestroy(x->graph);
-        x->graph = nullptr;
-    }
-    return CSU_OK;
+    return write_scalars_n(x, hs.data(), x->nsolve);
 }
 
-// Captures `iters` iterations into a graph (the DPLUR buffer parity returns to its start value).
-static int build_graph(csu_ctx* x, int iters)
+// Captures GRAPH_SIZES[gi] iterations into a graph starting at the current DPLUR buffer parity.
+static int build_graph(csu_ctx* x, int gi)
 {
-    if (x->graph) {
-        cudaGraphExecDestroy(x->graph);
-        x->graph = nullptr;
+    const int q = x->xcur;
+    if (x->graphs[gi][q]) {
+        cudaGraphExecDestroy(x->graphs[gi][q]);
+        x->graphs[gi][q] = nullptr;
     }
-    int xcur0 = x->xcur;
     long long l0 = x->launches;
     cudaGraph_t g;
     CK(cudaStreamBeginCapture(x->stream, cudaStreamCaptureModeThreadLocal));
-    for (int i = 0; i < iters; i++) DISPATCH(launch_iteration, x);
+    for (int i = 0; i < GRAPH_SIZES[gi]; i++) DISPATCH(launch_iteration, x);
     cudaError_t e = cudaStreamEndCapture(x->stream, &g);
     if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
-    e = cudaGraphInstantiate(&x->graph, g, 0);
+    e = cudaGraphInstantiate(&x->graphs[gi][q], g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
-    x->graph_iters = iters;
-    x->graph_launches = x->launches - l0;
-    x->xcur = xcur0;
+    x->graph_launches[gi][q] = x->launches - l0;
+    x->xcur = q;
     x->launches = l0;
     return CSU_OK;
 }
 
-static int run_iterations(csu_ctx* x, int n, int it0, Scalars* out)
+// Start of a call on the device: history rows and the call's iteration count restart; a one-solve context
+// also restarts its loop counter at it0 (the solves of a pack keep their own).
+__global__ void k_call_begin(Scalars* sc, int n, int it0, int set_iter)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    sc[k].hist_row = 0;
+    sc[k].steps = 0;
+    if (set_iter) sc[k].iter = it0;
+}
+
+// The parity the DPLUR increment buffers have after `iters` iterations from parity q.
+static int parity_after(const csu_ctx* x, int q, int iters)
+{
+    const int flips = x->cfg.time_scheme == CSU_TS_DPLUR ? x->cfg.n_linear * iters : 0;
+    return q ^ (flips & 1);
+}
+
+// n iterations on the device: graphs of 8, 4, 2 and 1 iterations replayed largest first, nothing waited on
+// before the launches; the scalars of solve 0 (and its history rows, when asked) come back at the end in
+// one synchronization. One-solve contexts capture all four graphs the first time they need one (a later
+// call of another length then replays without capturing); packs capture the ones their calls use.
+static int run_iterations(csu_ctx* x, int n, int it0, Scalars* out, double* hist_rows)
 {
     int st;
     if ((st = ensure_hist(x, n))) return st;
+    if (!x->h_sc) CK(cudaMallocHost((void**)&x->h_sc, sizeof(Scalars)));
     if (!x->prepared && !x->is_pack) {
         if ((st = reset_scalars(x, it0))) return st;
     } else {
-        // keep the device step state, restart the history rows (and, for one solve, the loop counter;
-        // the solves of a pack keep their own)
-        std::vector<Scalars> hs(x->nsolve);
-        if ((st = read_scalars_n(x, hs.data(), x->nsolve))) return st;
-        for (Scalars& h : hs) {
-            h.hist_row = 0;
-            if (!x->is_pack) h.iter = it0;
-            h.steps = 0;
-        }
-        if ((st = write_scalars_n(x, hs.data(), x->nsolve))) return st;
+        k_call_begin<<<(x->nsolve + 31) / 32, 32, 0, x->stream>>>(x->st.sc, x->nsolve, it0, x->is_pack ? 0 : 1);
+        x->launches++;
     }
     if (!x->prepared) {
         DISPATCH(launch_prologue, x);
         if ((st = check_launch("prologue"))) return st;
         x->prepared = 1;
     }
-    // graphs of G iterations; G even so the DPLUR increment buffers come back to the same parity
-    const int G = 8;
-    int done = 0;
-    if (n >= G) {
-        if (!x->graph || x->graph_iters != G)
-            if ((st = build_graph(x, G))) return st;
-        while (n - done >= G) {
-            CK(cudaGraphLaunch(x->graph, x->stream));
-            x->launches += x->graph_launches;
-            done += G;
+    if (!x->is_pack) {
+        // every size at the parities this context can start a graph with
+        for (int gi = 0; gi < 4; gi++)
+            if (!x->graphs[gi][x->xcur])
+                if ((st = build_graph(x, gi))) return st;
+    }
+    int left = n;
+    for (int gi = 0; gi < 4; gi++) {
+        while (left >= GRAPH_SIZES[gi]) {
+            const int q = x->xcur;
+            if (!x->graphs[gi][q])
+                if ((st = build_graph(x, gi))) return st;
+            CK(cudaGraphLaunch(x->graphs[gi][q], x->stream));
+            x->launches += x->graph_launches[gi][q];
+            x->xcur = parity_after(x, q, GRAPH_SIZES[gi]);
+            left -= GRAPH_SIZES[gi];
         }
     }
-    for (; done < n; done++) DISPATCH(launch_iteration, x);
     if ((st = check_launch("iteration"))) return st;
-    if ((st = read_scalars(x, out))) return st;
+    CK(cudaMemcpyAsync(x->h_sc, x->st.sc, sizeof(Scalars), cudaMemcpyDeviceToHost, x->stream));
+    if (hist_rows && x->h_hist)
+        CK(cudaMemcpyAsync(x->h_hist, x->hist, sizeof(double) * (size_t)n * (x->nv + 4), cudaMemcpyDeviceToHost,
+                           x->stream));
+    CK(cudaStreamSynchronize(x->stream));
+    *out = *x->h_sc;
+    if (hist_rows && x->h_hist) {
+        const int rows = out->hist_row < n ? out->hist_row : n;
+        memcpy(hist_rows, x->h_hist, sizeof(double) * (size_t)rows * (x->nv + 4));
+    }
     return CSU_OK;
 }
 
@@ -1101,14 +1161,10 @@ extern "C" int csu_iterate_ex(csu_ctx* x, int n, int it0, double* hist, int* n_d
     if (n_done) *n_done = 0;
     if (n == 0) return CSU_OK;
     Scalars h;
-    int st = run_iterations(x, n, it0, &h);
+    int st = run_iterations(x, n, it0, &h, x->is_pack ? nullptr : hist);
     if (!st && n_done) *n_done = h.steps;
     if (st) return st;
     if (x->is_pack) return CSU_OK; // per-solve results: csu_pack_info, csu_pack_history
-    if (hist) {
-        int rows = h.hist_row < n ? h.hist_row : n;
-        CK(cudaMemcpy(hist, x->hist, sizeof(double) * (size_t)rows * (x->nv + 4), cudaMemcpyDeviceToHost));
-    }
     if (h.status) {
         csu_set_error("csu_iterate: state became non-finite at iteration %d", h.iter);
         return h.status;
@@ -1134,23 +1190,17 @@ extern "C" int csu_tube_run(csu_ctx* x, double tmax, int* steps, double* t_final
     int st0 = upload_prm(x);
     if (st0) return st0;
     x->prepared = 0;
-    if (x->graph) {
-        cudaGraphExecDestroy(x->graph);
-        x->graph = nullptr;
-    }
+    drop_graphs(x);
     Scalars h;
     int st, total = 0;
     memset(&h, 0, sizeof(h));
     // the loop of solver.c:1921-1940 runs until the step that reaches tmax; checked every 64 steps
     for (int guard = 0; guard < 20000; guard++) {
-        if ((st = run_iterations(x, 64, total, &h))) return st;
+        if ((st = run_iterations(x, 64, total, &h, nullptr))) return st;
         total = h.iter;
         if (h.done || h.status) break;
     }
-    if (x->graph) {
-        cudaGraphExecDestroy(x->graph);
-        x->graph = nullptr;
-    }
+    drop_graphs(x);
     *steps = total;
     *t_final = h.t;
     if (h.status) {
@@ -1344,7 +1394,7 @@ extern "C" int csu_time_kernels(csu_ctx* x, int iters, double* ms, int* count)
     }
     if (!x->prepared) {
         Scalars h;
-        if ((st = run_iterations(x, 1, 0, &h))) return st;
+        if ((st = run_iterations(x, 1, 0, &h, nullptr))) return st;
     }
     CK(cudaStreamSynchronize(x->stream));
     x->timing = true;
@@ -1457,6 +1507,16 @@ extern "C" int csu_pack_get_state(csu_ctx* x, int k, double* U)
 {
     if (!x || !U || k < 0 || k >= x->nsolve) return CSU_ERR_INPUT;
     return solve_state_io(x, k, U, false);
+}
+
+extern "C" int csu_pack_stop(csu_ctx* x, int k)
+{
+    if (!x || k < 0 || k >= x->nsolve) return CSU_ERR_INPUT;
+    // done = 3: every kernel skips the solve from the next launch on, like a converged one
+    static const int stopped = 3;
+    CK(cudaMemcpyAsync(&x->st.sc[k].done, &stopped, sizeof(int), cudaMemcpyHostToDevice, x->stream));
+    CK(cudaStreamSynchronize(x->stream));
+    return CSU_OK;
 }
 
 static void solve_info_from(const csu_ctx* x, const Scalars& h, csu_solve_info* info)
@@ -1720,26 +1780,37 @@ __global__ void k_copy_jobs(const CopyJob* __restrict__ jobs, int n)
     }
 }
 
-// the device copy of a plan's job table, kept and grown across rebuilds (freed with the pack arenas)
+// the device copy of a plan's job table per device, kept and grown across rebuilds (freed with the pack
+// arenas)
+struct JobTable {
+    CopyJob* p = nullptr;
+    size_t cap = 0;
+};
+constexpr int MAX_JOB_DEVICES = 64;
 std::mutex g_jobs_mu;
-CopyJob* g_jobs_dev = nullptr;
-size_t g_jobs_cap = 0;
+JobTable g_jobs[MAX_JOB_DEVICES];
 
 static int run_copy_plan(csu_ctx* x, CopyPlan& plan)
 {
     if (plan.jobs.empty()) return CSU_OK;
-    std::lock_guard<std::mutex> lk(g_jobs_mu);
-    const size_t n = plan.jobs.size();
-    if (n > g_jobs_cap) {
-        if (g_jobs_dev) cudaFree(g_jobs_dev);
-        g_jobs_dev = nullptr;
-        g_jobs_cap = 0;
-        size_t cap = std::max(n, (size_t)4096);
-        CK(cudaMalloc((void**)&g_jobs_dev, sizeof(CopyJob) * cap));
-        g_jobs_cap = cap;
+    if (x->device < 0 || x->device >= MAX_JOB_DEVICES) {
+        csu_set_error("pack rebuild: device %d beyond the %d supported", x->device, MAX_JOB_DEVICES);
+        return CSU_ERR_UNSUPPORTED;
     }
-    CK(cudaMemcpyAsync(g_jobs_dev, plan.jobs.data(), sizeof(CopyJob) * n, cudaMemcpyHostToDevice, x->stream));
-    k_copy_jobs<<<(int)std::min(n, (size_t)(148 * 8)), 256, 0, x->stream>>>(g_jobs_dev, (int)n);
+    std::lock_guard<std::mutex> lk(g_jobs_mu);
+    JobTable& T = g_jobs[x->device];
+    const size_t n = plan.jobs.size();
+    if (n > T.cap) {
+        if (T.p) cudaFree(T.p);
+        T.p = nullptr;
+        T.cap = 0;
+        size_t cap = std::max(n, (size_t)4096);
+        CK(cudaMalloc((void**)&T.p, sizeof(CopyJob) * cap));
+        T.cap = cap;
+    }
+    CK(cudaMemcpyAsync(T.p, plan.jobs.data(), sizeof(CopyJob) * n, cudaMemcpyHostToDevice, x->stream));
+    // enough blocks to fill the device (8 per multiprocessor), never more than there are jobs
+    k_copy_jobs<<<(int)std::min(n, (size_t)x->sm_count * 8), 256, 0, x->stream>>>(T.p, (int)n);
     CK(cudaGetLastError());
     CK(cudaStreamSynchronize(x->stream)); // the table is reused by the next plan
     plan.jobs.clear();
@@ -1774,9 +1845,11 @@ static void state_copy_plan(csu_ctx* from, int kf, csu_ctx* to, int kt, CopyPlan
 static void release_copy_jobs()
 {
     std::lock_guard<std::mutex> lk(g_jobs_mu);
-    if (g_jobs_dev) cudaFree(g_jobs_dev);
-    g_jobs_dev = nullptr;
-    g_jobs_cap = 0;
+    for (JobTable& T : g_jobs) {
+        if (T.p) cudaFree(T.p);
+        T.p = nullptr;
+        T.cap = 0;
+    }
 }
 
 // The state copies of csu_pack_transfer, run at once.

@@ -9,8 +9,10 @@
 // The per-block partial sums live in a file-scope __device__ array (g_norm_scratch): every GPU that loads
 // the library holds it (192 KiB) until the process exits. Host code reaches it only through the address
 // returned by cudaGetSymbolAddress, looked up once per device on the first call made with that device
-// current. Calls share the array: two calls whose kernels overlap on a GPU race on it. Each call writes every
-// partial it later reads, so nothing has to be cleared between calls.
+// current and cached for the life of the process: after a cudaDeviceReset the device's module is loaded
+// again at another address, so the entry point must not be used across a device reset. Calls share the
+// array: two calls whose kernels overlap on a GPU race on it. Each call writes every partial it later reads,
+// so nothing has to be cleared between calls.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <mutex>
@@ -141,6 +143,12 @@ extern "C" int csu_residual_norms_noalloc(const double* R, int nvar, int ncells,
             }
         }
         scratch = g_scratch_ptr[dev];
+    }
+    // an error left by the caller's earlier work is reported as such, not as a failure of these launches
+    e = cudaPeekAtLastError();
+    if (e != cudaSuccess) {
+        csu_set_error("csu_residual_norms_noalloc: an earlier CUDA error is pending: %s", cudaGetErrorString(e));
+        return CSU_ERR_CUDA;
     }
     cudaStream_t s = (cudaStream_t)stream;
     k_norm_partial<<<(unsigned)nblocks, NA_BLOCK, 0, s>>>(R, nvar, ncells, scratch);

@@ -42,6 +42,7 @@ struct Group {
     std::vector<Req*> members; // in pack order (finished ones stay frozen until the next rebuild)
     std::vector<Req*> pending; // admitted, joining at the next rebuild
     int steps_since = 0;       // steps since the pack was built
+    bool drop_now = false;     // a member was cancelled: rebuild without it at the next step
 };
 
 // A submitted mesh, owned by the request while a preparation thread builds its layout.
@@ -94,7 +95,16 @@ struct Req {
     long long bytes = 0;
     Group* group = nullptr;   // the group whose pack holds it (frozen there once finished)
     bool taken = false;       // result taken while still frozen in a pack: freed at the rebuild
+    int status = CSU_OK;      // why it failed or stopped (CSU_ERR_*)
+    char message[192] = {0};  // the failure's message, kept with the request (errors of a preparation
+                              // thread are that thread's own csu_last_error)
 };
+
+void fail_req(Req* r, int status, const char* msg)
+{
+    r->status = status;
+    snprintf(r->message, sizeof(r->message), "%s", msg ? msg : "");
+}
 
 bool same_class(const csu_config& a, const csu_config& b)
 {
@@ -152,7 +162,13 @@ static void prepare(csu_srv* s, Req* r)
 {
     csu_prep* p = nullptr;
     int st = csu_prep_create(&r->mesh->d, &r->cfg, &p);
-    if (!st && csu_prep_bytes(p) > s->cfg.budget_bytes) {
+    if (st) {
+        fail_req(r, st, csu_last_error());
+    } else if (csu_prep_bytes(p) > s->cfg.budget_bytes) {
+        char msg[160];
+        snprintf(msg, sizeof(msg), "the solve needs %lld device bytes, more than the budget of %lld",
+                 csu_prep_bytes(p), s->cfg.budget_bytes);
+        fail_req(r, CSU_ERR_OOM, msg);
         csu_prep_destroy(p);
         p = nullptr;
         st = CSU_ERR_OOM;
@@ -255,6 +271,11 @@ static int retire(csu_srv* s, Group* g)
         if ((st = csu_pack_get_state(g->pack, (int)k, r->U.data()))) return st;
         r->state = fin;
         r->t_end = s->now();
+        if (fin == CSU_SRV_FAILED) {
+            char msg[96];
+            snprintf(msg, sizeof(msg), "the state became non-finite by iteration %d", info.iter);
+            fail_req(r, info.status, msg);
+        }
     }
     return CSU_OK;
 }
@@ -339,7 +360,11 @@ extern "C" int csu_srv_step(csu_srv* s, int* n_running, int* n_queued)
             ++it;
             continue;
         }
-        if (rd == 2) { // its layout failed or it exceeds the budget
+        if (r->state == CSU_SRV_CANCELLED) {
+            it = s->queue.erase(it);
+            continue;
+        }
+        if (rd == 2) { // its layout failed or it exceeds the budget (status and message set by prepare)
             r->state = CSU_SRV_FAILED;
             r->t_start = r->t_end = s->now();
             it = s->queue.erase(it);
@@ -363,7 +388,8 @@ extern "C" int csu_srv_step(csu_srv* s, int* n_running, int* n_queued)
     t = s->now();
     for (Group* g : s->groups) {
         bool idle = g->pack && active(g) == 0;
-        if (!g->pending.empty() || idle) {
+        if (!g->pending.empty() || idle || g->drop_now) {
+            g->drop_now = false;
             if ((st = rebuild(s, g))) return st;
             s->rebuilds++;
         }
@@ -405,6 +431,64 @@ extern "C" int csu_srv_info(csu_srv* s, long long id, csu_srv_request_info* out)
     out->t_start = r->t_start;
     out->t_end = r->t_end;
     out->n_cells = r->nc;
+    out->status = r->status;
+    return CSU_OK;
+}
+
+extern "C" int csu_srv_message(csu_srv* s, long long id, char* buf, int cap)
+{
+    if (!s || !buf || cap < 1) return CSU_ERR_INPUT;
+    auto it = s->reqs.find(id);
+    if (it == s->reqs.end()) {
+        csu_set_error("csu_srv_message: no request %lld", id);
+        return CSU_ERR_INPUT;
+    }
+    snprintf(buf, (size_t)cap, "%s", it->second->message);
+    return CSU_OK;
+}
+
+extern "C" int csu_srv_cancel(csu_srv* s, long long id)
+{
+    if (!s) return CSU_ERR_INPUT;
+    auto it = s->reqs.find(id);
+    if (it == s->reqs.end()) {
+        csu_set_error("csu_srv_cancel: no request %lld", id);
+        return CSU_ERR_INPUT;
+    }
+    Req* r = it->second;
+    if (r->state != CSU_SRV_QUEUED && r->state != CSU_SRV_RUNNING) {
+        csu_set_error("csu_srv_cancel: request %lld has already finished", id);
+        return CSU_ERR_STATE;
+    }
+    Group* g = r->group;
+    if (r->state == CSU_SRV_RUNNING && g) {
+        auto pit = std::find(g->pending.begin(), g->pending.end(), r);
+        if (pit != g->pending.end()) {
+            // admitted, not in a pack yet: its bytes go back now, its state is still the initial one
+            g->pending.erase(pit);
+            s->used -= r->bytes;
+            r->group = nullptr;
+        } else {
+            // in the pack: its state as it stands, then frozen there until the rebuild at the next step
+            auto mit = std::find(g->members.begin(), g->members.end(), r);
+            if (mit != g->members.end() && g->pack) {
+                const int k = (int)(mit - g->members.begin());
+                int st = csu_pack_stop(g->pack, k);
+                if (!st) st = csu_pack_get_state(g->pack, k, r->U.data());
+                if (!st) {
+                    csu_solve_info info;
+                    if (!(st = csu_pack_info(g->pack, k, &info))) r->iters = info.iter;
+                }
+                if (st) return st;
+            }
+            g->drop_now = true;
+        }
+    }
+    // a queued request leaves the queue at the next step (a preparation thread may still hold it)
+    r->state = CSU_SRV_CANCELLED;
+    r->t_end = s->now();
+    if (r->t_start == 0) r->t_start = r->t_end;
+    fail_req(r, CSU_ERR_CANCELLED, "cancelled by the caller");
     return CSU_OK;
 }
 
@@ -418,10 +502,17 @@ extern "C" int csu_srv_take(csu_srv* s, long long id, double* U)
         csu_set_error("csu_srv_take: request %lld has not finished", id);
         return CSU_ERR_STATE;
     }
+    // a request cancelled while a preparation thread builds its layout: wait for the thread to let go of it
+    while (r->ready.load(std::memory_order_acquire) == 0) std::this_thread::sleep_for(std::chrono::microseconds(200));
     if (U) memcpy(U, r->U.data(), sizeof(double) * r->U.size());
     s->reqs.erase(it);
-    if (r->group) r->taken = true; // still frozen in a pack: released when the pack is rebuilt
-    else delete r;
+    s->queue.erase(std::remove(s->queue.begin(), s->queue.end(), r), s->queue.end());
+    if (r->group) {
+        r->taken = true; // still frozen in a pack: released when the pack is rebuilt
+    } else {
+        if (r->prep) csu_prep_destroy(r->prep);
+        delete r;
+    }
     return CSU_OK;
 }
 

@@ -92,7 +92,8 @@ typedef struct csu_config {
 
 /*
  * The mesh as meshInit (mesh.c:115-266) leaves it, as plain arrays. A caller holding the reference's
- * MESH* fills it directly; csu_case_load builds the same arrays from a case folder.
+ * MESH* fills it directly (con from mesh->con, cell_faces from ELEMENT.f, cell_nei from ELEMENT.neiL, the
+ * boundary faces from mesh->bc[m]->elem); csu_case_load builds the same arrays from a case folder.
  */
 typedef struct csu_mesh_desc {
     int n_points;
@@ -230,8 +231,10 @@ int csu_time_kernels(csu_ctx* ctx, int iters, double* ms, int* count);
  * device-memory budget under their own allocator or must not call cudaMalloc/cudaFree (which synchronize
  * the device). Its scratch is a fixed array inside the library, held by every GPU that loads it (192 KiB);
  * ncells is limited to 8,388,608 (CSU_ERR_INPUT beyond). The first call on a device looks the scratch
- * address up (cudaGetSymbolAddress) and should come before any stream capture on that device. Calls
- * whose kernels overlap on one GPU share the scratch and race. */
+ * address up (cudaGetSymbolAddress) and should come before any stream capture on that device; the address
+ * is kept for the process, so the entry must not be used across a cudaDeviceReset. Calls whose kernels
+ * overlap on one GPU share the scratch and race. A CUDA error already pending from earlier work is returned
+ * (CSU_ERR_CUDA) before anything is launched. */
 int csu_residual_norms_noalloc(const double* R, int nvar, int ncells, double* res, void* stream);
 
 /* Counters of the engine: kernels launched since creation, device bytes held. */
@@ -250,7 +253,8 @@ typedef struct csu_prep csu_prep;
 typedef struct csu_solve_info {
     int iter;        /* iterations done (the solve's own counter)                  */
     int status;      /* CSU_OK or CSU_ERR_NONFINITE                                 */
-    int done;        /* 1: the residual-drop stop (convDrop) was reached; 2: iterCap */
+    int done;        /* 1: the residual-drop stop (convDrop) was reached; 2: iterCap; 3: stopped by
+                        csu_pack_stop                                                */
     int hist_rows;   /* history rows recorded by the last csu_iterate call          */
     int have_res0;   /* res0 holds the first residual                              */
     double res0[6];  /* RMS residuals of the solve's first iteration               */
@@ -270,6 +274,9 @@ int csu_pack_info(csu_ctx* ctx, int k, csu_solve_info* info);
 int csu_pack_infos(csu_ctx* ctx, csu_solve_info* infos);        /* all solves, one device read */
 int csu_pack_history(csu_ctx* ctx, int k, double* hist, int max_rows, int* rows);
 int csu_pack_transfer(csu_ctx* from, int k_from, csu_ctx* to, int k_to);
+/* Freezes solve k of a pack where it stands (done = 3): the pack's next iterations leave it unchanged while
+ * the other solves go on as before. The serving layer's cancellation uses it. */
+int csu_pack_stop(csu_ctx* ctx, int k);
 /* A new pack of `solves` in which solve k, when keep[k] >= 0, is solve keep[k] of `old` (mesh rows and
  * iteration state copied on the device, nothing re-uploaded); the others come from their host layouts and
  * need csu_pack_set_state. `old` is left unchanged (destroy it afterwards). */
@@ -288,6 +295,7 @@ int csu_pack_rebuild(csu_ctx* old, const int* keep, const csu_prep* const* solve
 #define CSU_SRV_CONVERGED 2
 #define CSU_SRV_FAILED 3
 #define CSU_SRV_MAXITER 4
+#define CSU_SRV_CANCELLED 5
 typedef struct csu_srv csu_srv;
 typedef struct csu_srv_config {
     long long budget_bytes;  /* device bytes the running solves may take                      */
@@ -308,6 +316,8 @@ typedef struct csu_srv_request_info {
     int n_cells;
     double drop;             /* RMS rho-residual / its first value                             */
     double t_submit, t_start, t_end;
+    int status;              /* CSU_OK, or why it failed or stopped: CSU_ERR_OOM (over the budget),
+                                CSU_ERR_INPUT (its layout failed), CSU_ERR_NONFINITE, CSU_ERR_CANCELLED */
 } csu_srv_request_info;
 
 int csu_srv_create(const csu_srv_config* cfg, csu_srv** out);
@@ -316,6 +326,13 @@ int csu_srv_submit(csu_srv* s, const csu_mesh_desc* mesh, const csu_config* cfg,
 int csu_srv_step(csu_srv* s, int* n_running, int* n_queued);
 int csu_srv_info(csu_srv* s, long long id, csu_srv_request_info* out);
 int csu_srv_take(csu_srv* s, long long id, double* U);      /* final state (reference order); forgets it */
+/* Cancels a queued or running request (CSU_ERR_STATE once it has finished). A queued one never starts; a
+ * running one stops where it stands (csu_srv_take returns that state) and its pack is rebuilt without it at
+ * the next csu_srv_step; the other solves' iterations are not affected. Its state becomes
+ * CSU_SRV_CANCELLED and its status CSU_ERR_CANCELLED. */
+int csu_srv_cancel(csu_srv* s, long long id);
+/* The message of a failed or cancelled request (also for failures met on a preparation thread). */
+int csu_srv_message(csu_srv* s, long long id, char* buf, int cap);
 int csu_srv_totals(csu_srv* s, long long* solve_iterations, long long* cell_updates, long long* used_bytes);
 /* host seconds spent rebuilding packs, iterating and polling, and the number of rebuilds */
 int csu_srv_times(csu_srv* s, double* rebuild_s, double* iterate_s, double* poll_s, int* rebuilds);

@@ -8,7 +8,7 @@ ref_<name>.npz
     oracle/Makefile) on those cases: the first residual at a fixed sample of cells and its RMS per
     variable, and the full-precision history (res[Nvar], Cx_p, Cx_v, Cy_p, Cy_v) of the first iterations.
 
-    python tests/golden/make_golden.py [/root/reference]
+    CSU_REFERENCE_DIR=<reference source tree> python tests/golden/make_golden.py [<reference source tree>]
 """
 import gzip
 import os
@@ -58,6 +58,8 @@ def make_vectors(names):
 
 
 if __name__ == "__main__":
-    ref_root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref_root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("CSU_REFERENCE_DIR")
+    if not ref_root:
+        sys.exit("make_golden.py: name the reference source tree (argument or CSU_REFERENCE_DIR)")
     names = copy_cases(ref_root)
     make_vectors(names)

@@ -49,6 +49,27 @@ def test_generated_meshes_integer_exact(native):
         assert np.array_equal(case.bface.ravel(), m["bface"])
 
 
+def test_bench_mesh_integer_exact(native):
+    """The benchmarked mesh at full size (160,000-cell jittered ramp): face list and order, neighbour
+    order, signed face lists, boundary faces identical to meshInit's (mesh.c:115-266)."""
+    import bench
+    import csu_b200
+    wd = bench.make_case(1, "int")
+    case = csu_b200.Case.load(wd)
+    ref = _ref(wd)
+    m = ref.mesh()
+    assert (case.n_cells, case.n_faces, case.n_bfaces) == (ref.nc, ref.nf, ref.nb) == (160000, 239400, 1200)
+    assert np.array_equal(case.con.ravel(), m["con"])
+    assert np.array_equal(case.cell_nodes.ravel(), m["nodes"])
+    assert np.array_equal(case.cell_faces.ravel(), m["f"])
+    assert np.array_equal(case.cell_nint, m["nint"])
+    assert np.array_equal(case.cell_nei.ravel(), m["nei"])
+    assert np.array_equal(case.bface.ravel(), m["bface"])
+    assert np.array_equal(case.marker_flag, m["marker_flag"])
+    assert np.array_equal(case.xy.ravel(), m["xy"])
+    assert np.array_equal(case.initial_state(), ref.get_U())
+
+
 def _ref_input(path):
     """The reference's own keyword parser, inputInit (input.c:7-95), through the built reference."""
     from oracle.refharness import LIB, available
