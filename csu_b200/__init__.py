@@ -23,7 +23,7 @@ ERRORS = {
     6: "CSU_ERR_CANCELLED", 7: "CSU_ERR_CUDA", 8: "CSU_ERR_UNSUPPORTED", 9: "CSU_ERR_STATE",
     10: "CSU_ERR_NO_DEVICE",
 }
-DUMP = {"P": 1, "GHOST_P": 2, "GRAD": 3, "PHI": 4, "FACEFLUX": 5, "R": 6, "D": 7, "DTL": 8, "DW": 9, "BLOCKS": 10, "LSQ_X87": 11, "SST_JAC": 12}
+DUMP = {"P": 1, "GHOST_P": 2, "GRAD": 3, "PHI": 4, "FACEFLUX": 5, "R": 6, "D": 7, "DTL": 8, "DW": 9, "BLOCKS": 10, "LSQ_X87": 11, "SST_JAC": 12, "BVISC": 13}
 FLUX = {"ROE": 0, "AUSM": 1, "AUSMDV": 2, "AUSMpup": 3, "AUSMpup2": 4}
 BC = {"symmetry": 0, "inlet": 1, "outlet": 2, "wall": 3, "wallT": 4}
 
@@ -281,7 +281,7 @@ class Engine:
         nc, nv, nf, nb = self.n_cells, self.nvar, self.case.n_faces, self.case.n_bfaces
         shapes = {"P": (nc, nv + 1), "GHOST_P": (nb, nv + 1), "GRAD": (2, nv, nc), "PHI": (nv, nc),
                   "FACEFLUX": (nv, nf), "R": (nv, nc), "D": (nc,), "DTL": (nc,), "DW": (nv, nc),
-                  "BLOCKS": (nc, 4, nv, nv), "LSQ_X87": (1,), "SST_JAC": (6, nc)}
+                  "BLOCKS": (nc, 4, nv, nv), "LSQ_X87": (1,), "SST_JAC": (6, nc), "BVISC": (nb, 4)}
         out = np.zeros(shapes[what])
         _check(lib().csu_dump(self._h, DUMP[what], _ptr(out)))
         return out

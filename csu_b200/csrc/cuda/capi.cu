@@ -1357,6 +1357,18 @@ extern "C" int csu_dump(csu_ctx* x, int what, double* out)
             for (int c = 0; c < nc; c++) out[(size_t)q * nc + n2o[c]] = a[(size_t)q * nc + c];
         return CSU_OK;
     }
+    case CSU_DUMP_BVISC: {
+        if (!x->prm.visc) {
+            csu_set_error("csu_dump: no viscous fluxes in this context (laminar, SA or SST only)");
+            return CSU_ERR_STATE;
+        }
+        CK(d2h(a, x->st.FV + nf, (size_t)4 * nb));
+        for (int b = 0; b < nb; b++) {
+            double* o = out + (size_t)x->L.bold[b] * 4;
+            for (int k = 0; k < 4; k++) o[k] = a[(size_t)4 * b + k];
+        }
+        return CSU_OK;
+    }
     case CSU_DUMP_LSQ_X87: {
         unsigned long long q = 0;
         CK(cudaMemcpy(&q, x->st.lsq_x87, sizeof(q), cudaMemcpyDeviceToHost));

@@ -8,11 +8,15 @@
  *   solution.csv     node values of U by inverse-distance weighting of the cells (solver.c:222-325)
  *   solution2.csv    node values of primitives, Mach, H, entropy (solver.c:2009-2220)
  *   restart.csv      cell values of U (solver.c:327-355), after the primitive clamps of solution2
- *   surfData.csv     laminar wall data along the `writeSurf` marker (laminar.c:350-492)
+ *   surfData.csv     wall data along the `writeSurf` marker (laminar.c:350-492, sa.c:854-996,
+ *                    saCC.c:599-745, sst.c:820-962; dispatched as solverWriteSurf, solver.c:1984-2007)
  *
  * The iteration history comes from the device (csu_iterate). Node interpolation and file writing stay on
- * the host: they run once per solve. friction.csv and surfData.csv use the gradients of the last residual
- * evaluation and the primitives of the final state.
+ * the host: they run once per solve. friction.csv and surfData.csv are written, as in the reference, from
+ * what the last iteration's residual evaluation left: primitives, ghost states and gradients of the state
+ * that iteration started from (the reference never recomputes them after its last update). The engine
+ * therefore runs Nmax - 1 iterations, evaluates the residual of that state once (csu_residual: it leaves
+ * exactly those arrays on the device), writes the two files, and runs the last iteration.
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -180,7 +184,147 @@ static int write_restart(const char* wd, const csu_case* cs, const double* U)
     return CSU_OK;
 }
 
-/* boundaryCalcTensorWall (boundary.c:744-794) per wall face, from the owner's gradients and primitives */
+/* meshCalcDS (mesh.c:720-740): face normal of the edge p0 -> p1, times the mean y when axisymmetric */
+static void face_ds(const csu_mesh* m, int axi, int p0, int p1, double* dSx, double* dSy)
+{
+    double x0 = m->xy[2 * p0], y0 = m->xy[2 * p0 + 1], x1 = m->xy[2 * p1], y1 = m->xy[2 * p1 + 1];
+    *dSx = y1 - y0;
+    *dSy = -(x1 - x0);
+    double y = (y0 + y1) / 2;
+    if (axi == 1) {
+        *dSx = (*dSx) * y;
+        *dSy = (*dSy) * y;
+    }
+}
+
+/* Eddy viscosity that saBoundaryFaceViscFlux (sa.c:370-692) reports for one boundary face: fv1 of
+ * saCalcFace (sa.c:273-290) times rho nt, from the inlet state (flag 1), the owner with the wall
+ * temperature and nt = 0 (flag 4), the owner (flags 0, 2); 0 on adiabatic walls (flag 3). */
+static double sa_face_eddy(const csu_config* c, int flag, const double* E)
+{
+    if (flag == CSU_BC_WALL) return 0.0;
+    double rho = E[0], T = E[4], n = E[5];
+    if (flag == CSU_BC_INLET) {
+        rho = c->pin[0];
+        T = c->pin[4];
+        n = c->pin[5];
+    } else if (flag == CSU_BC_WALLT) {
+        T = c->t_wall;
+        n = 0.0;
+    }
+    double mi_L = csu_host_sutherland(T);
+    double n_L = mi_L / rho;
+    double Cv1 = 7.1;
+    double X = n / n_L;
+    double aux = X * X * X;
+    double fv1 = aux / (aux + Cv1 * Cv1 * Cv1);
+    return fv1 * rho * n;
+}
+
+/* The surface writers of the viscous models, along the marker named by writeSurf (default "wall"; solver.c:
+ * 1585-1594). Per boundary face: the ghost primitives of the last residual evaluation (boundary element P),
+ * pressure coefficient, skin friction and heat flux from the face's viscous flux (components 1..3 of
+ * boundaryFaceViscFlux and its SA/SST variants), y+ from the owner's wall distance, Mach; then each node of
+ * the marker gets the mean of its faces. Columns the reference leaves undefined are written as 0: the
+ * 'n' column of the laminar model (it reads past the five primitives of a boundary element), y+ of the
+ * laminar model (the wall distance is never computed), 'q' of adiabatic laminar walls (the energy
+ * component of the flux is never set), miEddy of SST (never set). */
+static int write_surf(const char* wd, const csu_case* cs, const double* ghost, const double* bvisc,
+                      const double* P)
+{
+    const csu_mesh* m = &cs->mesh;
+    const csu_config* c = &cs->cfg;
+    const int npr = c->nvar + 1;
+    const char* target = csu_keywords_get(&cs->kw, "writeSurf");
+    if (!target) target = "wall";
+    FILE* f = open_in(wd, "surfData.csv", "w");
+    if (!f) {
+        csu_set_error("cannot write %ssurfData.csv", wd);
+        return CSU_ERR_IO;
+    }
+    const double rin = c->pin[0], uin = c->pin[1], vin = c->pin[2], pin = c->pin[3];
+    const double qdin = 0.5 * rin * (uin * uin + vin * vin);
+    const int turb = c->sa || c->sst;
+    const int nq = turb ? 13 : 12;
+    int b0 = 0;
+    for (int k = 0; k < m->n_markers; b0 += m->marker_nbf[k], k++) {
+        if (strcmp(m->marker_name[k], target) != 0) continue;
+        if (turb) fprintf(f, "x,y,rho,u,v,p,T,n,Cp,Cfx,Cfy,q,yplus,mach,miEddy,\n");
+        else fprintf(f, "x,y,rho,u,v,p,T,n,Cp,Cfx,Cfy,q,yplus,mach,\n");
+        const int ne = m->marker_nbf[k], flag = m->marker_flag[k];
+        if (ne == 0) continue;
+        double* D = calloc((size_t)nq * ne, sizeof(double));
+        double* Dp = calloc((size_t)nq * (ne + 1), sizeof(double));
+        int* d = calloc(ne + 1, sizeof(int));
+        int* pn = calloc(ne + 1, sizeof(int));
+        int* pn2 = calloc(m->n_points, sizeof(int));
+        for (int i = 0; i < ne; i++) pn[i] = m->bface[3 * (b0 + i)];
+        pn[ne] = m->bface[3 * (b0 + ne - 1) + 1];
+        for (int i = 0; i < ne + 1; i++) pn2[pn[i]] = i;
+        for (int i = 0; i < ne; i++) {
+            const int b = b0 + i, p0 = m->bface[3 * b], p1 = m->bface[3 * b + 1], own = m->bface[3 * b + 2];
+            double dSx, dSy;
+            face_ds(m, c->axisymmetric, p0, p1, &dSx, &dSy);
+            double dS = sqrt(dSx * dSx + dSy * dSy);
+            const double* G = ghost + (size_t)b * npr;
+            const double* fv = bvisc + (size_t)b * 4;
+            double r = G[0], u = G[1], v = G[2], p = G[3], T = G[4];
+            double Cp = (p - pin) / qdin;
+            double Cfx = fv[0] / (dS * qdin);
+            double Cfy = fv[1] / (dS * qdin);
+            double q = (fv[2] - u * fv[0] - v * fv[1]) / dS;
+            double tau = sqrt(fv[0] * fv[0] + fv[1] * fv[1]) / dS;
+            double uplus = sqrt(tau / r);
+            double dwall = m->wall_dist ? m->wall_dist[own] : 0.0;
+            double yplus = fabs(r * uplus * dwall) / csu_host_sutherland(T);
+            double cc = csu_host_T2c(c, T);
+            double mach = sqrt(u * u + v * v) / cc;
+            if (!turb && flag == CSU_BC_WALL) q = 0.0;
+            double* col = D + i;
+            col[0 * ne] = r;
+            col[1 * ne] = u;
+            col[2 * ne] = v;
+            col[3 * ne] = p;
+            col[4 * ne] = T;
+            col[5 * ne] = turb ? G[5] : 0.0;
+            col[6 * ne] = Cp;
+            col[7 * ne] = Cfx;
+            col[8 * ne] = Cfy;
+            col[9 * ne] = q;
+            col[10 * ne] = yplus;
+            col[11 * ne] = mach;
+            if (turb) col[12 * ne] = c->sa ? sa_face_eddy(c, flag, P + (size_t)own * npr) : 0.0;
+        }
+        for (int i = 0; i < ne; i++) {
+            const int b = b0 + i, p0 = m->bface[3 * b], p1 = m->bface[3 * b + 1];
+            for (int q = 0; q < nq; q++) {
+                Dp[(size_t)q * (ne + 1) + pn2[p0]] += D[(size_t)q * ne + i];
+                Dp[(size_t)q * (ne + 1) + pn2[p1]] += D[(size_t)q * ne + i];
+            }
+            d[pn2[p0]] += 1;
+            d[pn2[p1]] += 1;
+        }
+        for (int i = 0; i < ne + 1; i++)
+            for (int q = 0; q < nq; q++) Dp[(size_t)q * (ne + 1) + i] /= d[i];
+        for (int i = 0; i < ne + 1; i++) {
+            fprintf(f, "% .10e,", m->xy[2 * pn[i]]);
+            fprintf(f, "% .10e,", m->xy[2 * pn[i] + 1]);
+            for (int q = 0; q < nq; q++) fprintf(f, "% .10e,", Dp[(size_t)q * (ne + 1) + i]);
+            fprintf(f, "\n");
+        }
+        free(D);
+        free(Dp);
+        free(d);
+        free(pn);
+        free(pn2);
+    }
+    fclose(f);
+    return CSU_OK;
+}
+
+/* solverCalcCoeff2 (solver.c:1303-1340) per wall face, from the owner's gradients and primitives:
+ * boundaryCalcTensorWall (boundary.c:744-794) for the laminar model, saCalcTensorWall (sa.c:795-852: the
+ * wall-tangent shear in the txy column, zeros beside it, y+ from the wall distance) for SA and SST. */
 static int write_friction(const char* wd, const csu_case* cs, const double* P, const double* G)
 {
     const csu_mesh* m = &cs->mesh;
@@ -213,6 +357,18 @@ static int write_friction(const char* wd, const csu_case* cs, const double* P, c
             double txx = 2 * mi * (dux - (dux + dvy) / 3);
             double tyy = 2 * mi * (dvy - (dux + dvy) / 3);
             double txy = mi * (duy + dvx);
+            if (c->sa || c->sst) {
+                double dSx, dSy;
+                face_ds(m, c->axisymmetric, p0, p1, &dSx, &dSy);
+                double dS = sqrt(dSx * dSx + dSy * dSy);
+                double fx = (txx * dSx + txy * dSy) / dS;
+                double fy = (txy * dSx + tyy * dSy) / dS;
+                double ft = (fx * dSy - fy * dSx) / dS;
+                double ut = sqrt(fabs(ft) / E[0]);
+                double dwall = m->wall_dist ? m->wall_dist[e0] : 0.0;
+                fprintf(f, "%e, %e, %e, %e, %e,\n", x1, 0.0, ft, 0.0, E[0] * dwall * ut / mi);
+                continue;
+            }
             double aux = 5.29 * x1 / sqrt(E[0] * E[1] * x1 / mi);
             fprintf(f, "%e, %e, %e, %e, %e,\n", x1, txx, txy, tyy, L / aux);
         }
@@ -232,6 +388,7 @@ int csu_run_case(const char* wd, int verbose)
     const csu_config* c = &cs->cfg;
     int nc = d.n_cells, nv = c->nvar;
     double *U = NULL, *hist = NULL, *P = NULL, *G = NULL;
+    int wrote_wall = 0;
     FILE* conv = NULL;
     if ((st = csu_create(&d, c, &ctx))) goto done;
     U = malloc(sizeof(double) * (size_t)nv * nc);
@@ -250,10 +407,30 @@ int csu_run_case(const char* wd, int verbose)
             goto done;
         }
         const int chunk = 1000;
+        const int visc = c->laminar || c->sa || c->sst;
         hist = malloc(sizeof(double) * (size_t)chunk * (nv + 4));
         if (verbose) printf("\nmain: running solution:\n");
-        for (int it = 0; it < nmax; it += chunk) {
+        for (int it = 0; it < nmax;) {
             int n = nmax - it < chunk ? nmax - it : chunk;
+            if (visc && it + n == nmax) {
+                if (n > 1) n--;
+                else {
+                    /* the last iteration: first the wall files from the state it starts from */
+                    double *GP = malloc(sizeof(double) * (size_t)(nv + 1) * (d.n_bfaces > 0 ? d.n_bfaces : 1));
+                    double *BV = malloc(sizeof(double) * (size_t)4 * (d.n_bfaces > 0 ? d.n_bfaces : 1));
+                    st = csu_residual(ctx, NULL);
+                    if (!st) st = csu_dump(ctx, CSU_DUMP_GRAD, G);
+                    if (!st) st = csu_dump(ctx, CSU_DUMP_P, P);
+                    if (!st) st = csu_dump(ctx, CSU_DUMP_GHOST_P, GP);
+                    if (!st) st = csu_dump(ctx, CSU_DUMP_BVISC, BV);
+                    if (!st) st = write_friction(wd, cs, P, G);
+                    if (!st) st = write_surf(wd, cs, GP, BV, P);
+                    free(GP);
+                    free(BV);
+                    if (st) goto done;
+                    wrote_wall = 1;
+                }
+            }
             if ((st = csu_iterate(ctx, n, it, hist))) goto done;
             for (int r = 0; r < n; r++) {
                 const double* h = hist + (size_t)r * (nv + 4);
@@ -267,11 +444,15 @@ int csu_run_case(const char* wd, int verbose)
                 fprintf(conv, " %e, %e, %e, %e,", h[nv], h[nv + 1], h[nv + 2], h[nv + 3]);
                 fprintf(conv, "\n");
             }
+            it += n;
         }
         fclose(conv);
         conv = NULL;
-        if ((st = csu_dump(ctx, CSU_DUMP_GRAD, G)) || (st = csu_dump(ctx, CSU_DUMP_P, P))) goto done;
-        if ((st = write_friction(wd, cs, P, G))) goto done;
+        if (!wrote_wall) {
+            /* inviscid (friction.csv holds no rows) or Nmax = 0 */
+            if ((st = csu_dump(ctx, CSU_DUMP_GRAD, G)) || (st = csu_dump(ctx, CSU_DUMP_P, P))) goto done;
+            if ((st = write_friction(wd, cs, P, G))) goto done;
+        }
     } else {
         double tmax, t = 0;
         int steps = 0;

@@ -88,9 +88,12 @@ def _ccw(points, cells):
 
 
 def _flow_kv(mach, pressure, temperature, alpha_deg=0.0):
+    """Free stream; the outlet back pressure `pout` is the free-stream pressure (the reference's default,
+    1e5 Pa, solver.c:1558-1565, would impose a wrong back pressure on cases run at another pressure, such
+    as the low-Reynolds ones whose pressure is set by the Reynolds number)."""
     a = math.radians(alpha_deg)
     return {"pressure": "%.17g" % pressure, "temperature": "%.17g" % temperature, "mach": "%.17g" % mach,
-            "nx": "%.17g" % math.cos(a), "ny": "%.17g" % math.sin(a)}
+            "nx": "%.17g" % math.cos(a), "ny": "%.17g" % math.sin(a), "pout": "%.17g" % pressure}
 
 
 def _solver_kv(flux="AUSMDV", order=1, scheme="DPLUR", n_linear=4, cfl=5.0, nmax=1000, viscous=None):
@@ -317,6 +320,8 @@ def ramp(ni=400, nj=200, length=1.5, x_ramp=0.5, angle_deg=15.0, height=1.0, jit
           "BC:wall": "wall", "Nmax": str(nmax), "order": str(order), "stages": "5", "threads": str(threads),
           "flux": flux, "tube": "0", "axisymmetric": "0", "CFL": "%g" % cfl, "timeScheme": scheme,
           "Nlinear": str(n_linear), "limK": "%g" % lim_k}
+    if pressure != 1e5:
+        kv["pout"] = "%.17g" % pressure  # the outlet back pressure at the free stream's (default 1e5 Pa)
     return su2, _input(kv)
 
 

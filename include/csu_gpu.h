@@ -191,7 +191,11 @@ int csu_tube_run(csu_ctx* ctx, double tmax, int* steps, double* t_final);
  *                                               least squares could not decide and left to the integer x87
  *                                               model (no reference counterpart: a diagnostic of this engine)
  *  CSU_DUMP_SST_JAC 6*ncells                    SST source Jacobians dQkdr, dQkdrk, dQkdro, dQodr, dQodrk,
- *                                               dQodro [6][cell] of the last LU-SGS iteration (sst.c:643-680) */
+ *                                               dQodro [6][cell] of the last LU-SGS iteration (sst.c:643-680)
+ *  CSU_DUMP_BVISC   nbfaces*4 [bface][k]        viscous flux of each boundary face: x and y momentum, energy,
+ *                                               transported scalar (components 1..4 of boundaryFaceViscFlux,
+ *                                               laminar.c:128-346; saBoundaryFaceViscFlux, sa.c:370-692;
+ *                                               sstBoundaryFaceViscFlux, sst.c:202-547); viscous models only */
 #define CSU_DUMP_P 1
 #define CSU_DUMP_GHOST_P 2
 #define CSU_DUMP_GRAD 3
@@ -204,6 +208,7 @@ int csu_tube_run(csu_ctx* ctx, double tmax, int* steps, double* t_final);
 #define CSU_DUMP_BLOCKS 10
 #define CSU_DUMP_LSQ_X87 11
 #define CSU_DUMP_SST_JAC 12
+#define CSU_DUMP_BVISC 13
 int csu_dump(csu_ctx* ctx, int what, double* out);
 
 /* Run the engine's work on a caller-provided cudaStream_t (NULL: the context's own stream). */

@@ -2,6 +2,8 @@
 the caller's state before upload, one poisoned solve in a pack, a request over the memory budget, a
 cancelled request. Each failure must be reported with its status (include/csu_gpu.h) while the rest of the
 work goes on exactly as it would without it."""
+import time
+
 import numpy as np
 import pytest
 
@@ -10,22 +12,27 @@ import casekit
 pytestmark = pytest.mark.gpu
 
 STRUCT = {"timeScheme": "DPLUR", "Nlinear": "4", "order": "1", "flux": "AUSMDV", "restart": "0"}
+# flow conditions the first-order DPLUR runs stably with (as in the serving tests)
+FLOW = {"caseWedge": {"CFL": "10.0"}, "caseCylinder": {"CFL": "4.0", "mach": "2.5"},
+        "caseWedgeQuad": {"CFL": "8.0", "mach": "2.2"}, "caseDiamond": {"CFL": "5.0"}}
 
 
 def _case(name, kv=None):
     import csu_b200
-    return csu_b200.Case.load(casekit.materialize(name, dict(STRUCT, **(kv or {}))))
+    return csu_b200.Case.load(casekit.materialize(name, dict(STRUCT, **FLOW[name], **(kv or {}))))
 
 
 def test_nonfinite_state_before_upload(native):
-    """NaN in one cell's density of the uploaded state: the first iteration after it reports
-    CSU_ERR_NONFINITE (status 4) with its iteration number, and no later iteration runs."""
+    """NaN in one cell's x momentum of the uploaded state: the first iteration after it reports
+    CSU_ERR_NONFINITE (status 4) with its iteration number, and no later iteration runs. (A NaN density or
+    energy would not do: the write-back clamps of solverCalcPrimitive, solver.c:1163-1202, are fmax calls,
+    which return rLim or the energy floor for a NaN operand, in the reference and here alike.)"""
     import csu_b200
     case = _case("caseWedge")
     eng = csu_b200.Engine(case)
     eng.iterate(3)
     U = eng.get_state()
-    U[0, case.n_cells // 2] = np.nan
+    U[1, case.n_cells // 2] = np.nan
     eng.set_state(U)
     with pytest.raises(csu_b200.CsuError) as e:
         eng.iterate(5, it0=3)
@@ -75,10 +82,10 @@ def test_request_over_budget(native, prep_threads):
         assert e.value.status == 3
     else:
         rid = srv.submit(case, max_iters=16)
-        for _ in range(200):
-            r, q = srv.step()
-            if srv.info(rid)["state"] != "queued":
-                break
+        t0 = time.time()
+        while srv.info(rid)["state"] == "queued" and time.time() - t0 < 60.0:
+            srv.step()
+            time.sleep(0.01)
         info = srv.info(rid)
         assert info["state"] == "failed" and info["status"] == 3
         assert "budget" in srv.message(rid)
