@@ -92,6 +92,7 @@ def lib():
         L.csu_iterate_ex.argtypes = [vp, C.c_int, C.c_int, vp, ip]
         L.csu_tube_run.argtypes = [vp, C.c_double, ip, dp]
         L.csu_dump.argtypes = [vp, C.c_int, vp]
+        L.csu_wall_data.argtypes = [vp]
         L.csu_stats.argtypes = [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
         L.csu_set_stream.argtypes = [vp, vp]
         L.csu_time_kernels.argtypes = [vp, C.c_int, dp, ip]

@@ -126,6 +126,8 @@ struct csu_ctx {
     cudaGraphExec_t graphs[4][2] = {};
     long long graph_launches[4][2] = {};
     Scalars* h_sc = nullptr;   // pinned: solve 0's scalars, read back once at the end of csu_iterate
+    int* h_flags = nullptr;    // pinned: halt flags (status, done) of two chunks in flight
+    cudaEvent_t ev_poll[2] = {nullptr, nullptr};
     double* h_hist = nullptr;  // pinned: solve 0's history rows (hist_cap rows)
     int have_debug = 0;
     cudaStream_t own_stream = nullptr;
@@ -164,6 +166,9 @@ static void tmark(csu_ctx* x, int kind)
 
 // iterations per captured graph; a call of n iterations replays the largest first (n = 8a + 4b + 2c + d)
 static const int GRAPH_SIZES[4] = {8, 4, 2, 1};
+// one-solve calls longer than this are launched in chunks of it, checking between chunks whether the solve
+// has halted
+static const int STOP_CHUNK = 64;
 
 static void drop_graphs(csu_ctx* x)
 {
@@ -690,6 +695,9 @@ extern "C" void csu_destroy(csu_ctx* x)
     if (x->hist) cudaFree(x->hist);
     if (x->h_sc) cudaFreeHost(x->h_sc);
     if (x->h_hist) cudaFreeHost(x->h_hist);
+    if (x->h_flags) cudaFreeHost(x->h_flags);
+    for (cudaEvent_t e : x->ev_poll)
+        if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : x->ev) cudaEventDestroy(e);
     if (x->own_stream) cudaStreamDestroy(x->own_stream);
     if (x->side) cudaStreamDestroy(x->side);
@@ -1129,16 +1137,45 @@ static int run_iterations(csu_ctx* x, int n, int it0, Scalars* out, double* hist
             if (!x->graphs[gi][x->xcur])
                 if ((st = build_graph(x, gi))) return st;
     }
-    int left = n;
-    for (int gi = 0; gi < 4; gi++) {
-        while (left >= GRAPH_SIZES[gi]) {
-            const int q = x->xcur;
-            if (!x->graphs[gi][q])
-                if ((st = build_graph(x, gi))) return st;
-            CK(cudaGraphLaunch(x->graphs[gi][q], x->stream));
-            x->launches += x->graph_launches[gi][q];
-            x->xcur = parity_after(x, q, GRAPH_SIZES[gi]);
-            left -= GRAPH_SIZES[gi];
+    auto launch_span = [&](int count) -> int {
+        for (int gi = 0; gi < 4; gi++) {
+            while (count >= GRAPH_SIZES[gi]) {
+                const int q = x->xcur;
+                int st2;
+                if (!x->graphs[gi][q])
+                    if ((st2 = build_graph(x, gi))) return st2;
+                CK(cudaGraphLaunch(x->graphs[gi][q], x->stream));
+                x->launches += x->graph_launches[gi][q];
+                x->xcur = parity_after(x, q, GRAPH_SIZES[gi]);
+                count -= GRAPH_SIZES[gi];
+            }
+        }
+        return CSU_OK;
+    };
+    if (x->is_pack || n <= STOP_CHUNK) {
+        if ((st = launch_span(n))) return st;
+    } else {
+        // A solve that halts (residual-drop stop, iteration cap, non-finite state) leaves the rest of the
+        // call's kernels with nothing to do, but they would still be launched. Chunks of STOP_CHUNK
+        // iterations instead, each followed by a copy of the halt flags; the host waits for the flags of the
+        // chunk before the one just enqueued, so the device always has a chunk queued while it looks.
+        if (!x->h_flags) CK(cudaMallocHost((void**)&x->h_flags, 4 * sizeof(int)));
+        for (int q = 0; q < 2; q++)
+            if (!x->ev_poll[q]) CK(cudaEventCreateWithFlags(&x->ev_poll[q], cudaEventDisableTiming));
+        int left = n;
+        for (int j = 0; left > 0; j++) {
+            const int c = left < STOP_CHUNK ? left : STOP_CHUNK;
+            if ((st = launch_span(c))) return st;
+            left -= c;
+            // status and done are adjacent in Scalars
+            CK(cudaMemcpyAsync(x->h_flags + 2 * (j & 1), &x->st.sc[0].status, 2 * sizeof(int),
+                               cudaMemcpyDeviceToHost, x->stream));
+            CK(cudaEventRecord(x->ev_poll[j & 1], x->stream));
+            if (j >= 1) {
+                CK(cudaEventSynchronize(x->ev_poll[(j - 1) & 1]));
+                const int* f = x->h_flags + 2 * ((j - 1) & 1);
+                if (f[0] | f[1]) break;
+            }
         }
     }
     if ((st = check_launch("iteration"))) return st;
@@ -1207,6 +1244,27 @@ extern "C" int csu_tube_run(csu_ctx* x, double tmax, int* steps, double* t_final
         csu_set_error("csu_tube_run: state became non-finite at step %d", total);
         return h.status;
     }
+    return CSU_OK;
+}
+
+extern "C" int csu_wall_data(csu_ctx* x)
+{
+    if (!x) return CSU_ERR_INPUT;
+    if (x->is_pack) {
+        csu_set_error("csu_wall_data: views in reference order are per solve and not available for packs");
+        return CSU_ERR_STATE;
+    }
+    if (x->L.nb == 0) return CSU_OK;
+    const int g = (x->L.nb + BLOCK - 1) / BLOCK;
+    switch (x->model) {
+    case 0: k_wall_data<0><<<g, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st); break;
+    case 1: k_wall_data<1><<<g, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st); break;
+    default: k_wall_data<2><<<g, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st); break;
+    }
+    x->launches++;
+    int st = check_launch("csu_wall_data");
+    if (st) return st;
+    CK(cudaStreamSynchronize(x->stream));
     return CSU_OK;
 }
 

@@ -485,6 +485,88 @@ __global__ void __launch_bounds__(BLOCK) k_grad_fix(const Prm* __restrict__ P, c
     }
 }
 
+// The owner's gradients a boundary face's viscous flux uses: u, v, T, then nt (SA) or k (SST), then the rho
+// gradient (SA: saCC's density terms) or omega (SST).
+template <int MODEL>
+__device__ __forceinline__ void owner_visc_gradients(const State& s, int nc, int c, double* gvx, double* gvy)
+{
+    double4 a = s.G4x[c], bb = s.G4y[c];
+    gvx[0] = a.y; gvx[1] = a.z; gvx[2] = s.GTx[c];
+    gvy[0] = bb.y; gvy[1] = bb.z; gvy[2] = s.GTy[c];
+    gvx[3] = MODEL >= 1 ? s.Gxx[c] : 0.0;
+    gvy[3] = MODEL >= 1 ? s.Gxy[c] : 0.0;
+    gvx[4] = MODEL == 2 ? s.Gxx[(size_t)nc + c] : (MODEL == 1 ? a.x : 0.0);
+    gvy[4] = MODEL == 2 ? s.Gxy[(size_t)nc + c] : (MODEL == 1 ? bb.x : 0.0);
+}
+
+// Viscous flux of boundary face b (device order; fi its slot in the face arrays) from its owner c's
+// primitives E0 and gradients: boundaryFaceViscFlux (laminar.c:128-346), saBoundaryFaceViscFlux (sa.c:370-692)
+// or its saCC variant, sstBoundaryFaceViscFlux (sst.c:202-547); stored in FV (and FV5) at fi.
+template <int MODEL>
+__device__ __forceinline__ void bface_visc(const Prm& p, const Mesh& m, const State& s, int b, int fi, int c,
+                                           int flag, double dSx, double dSy, const double* E0, const double* gvx,
+                                           const double* gvy, double2 bdv, double bLv)
+{
+    if constexpr (MODEL == 2) {
+        double2 un = m.bun[b];
+        double fv[5];
+        sst_boundary_flux(p.gas, p.sst_k, p.pr, p.pr_t, p.t_wall, p.pin, flag, gvx, gvy, E0, m.wall_d[c], dSx, dSy,
+                          bdv.x, bdv.y, bLv, un.x, un.y, m.bds2[b], fv);
+        s.FV[fi] = make_double4(fv[0], fv[1], fv[2], fv[3]);
+        s.FV5[fi] = fv[4];
+    } else if constexpr (MODEL == 1) {
+        double2 un = m.bun[b];
+        double fv[4];
+        if (p.sa_cc)
+            sacc_boundary_flux(p.gas, p.pr, p.pr_t, p.t_wall, p.pin, flag, gvx, gvy, E0, dSx, dSy, bdv.x, bdv.y,
+                               bLv, un.x, un.y, m.bds2[b], fv);
+        else
+            sa_boundary_flux(p.gas, p.pr, p.pr_t, p.t_wall, p.pin, flag, gvx, gvy, E0, dSx, dSy, bdv.x, bdv.y, bLv,
+                             un.x, un.y, m.bds2[b], fv);
+        s.FV[fi] = make_double4(fv[0], fv[1], fv[2], fv[3]);
+    } else {
+        if (p.laminar == 1) {
+            double2 un = m.bun[b];
+            double fv[3];
+            laminar_boundary(p.gas, p.pr, p.t_wall, p.pin, flag, gvx, gvy, E0, dSx, dSy, bdv.x, bdv.y, bLv, un.x,
+                             un.y, m.bds2[b], fv);
+            s.FV[fi] = make_double4(fv[0], fv[1], fv[2], 0.0);
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// k_wall_data: what the reference's surface writers read after its last iteration (solverWriteSolution2
+// recomputes the cell and ghost primitives of the final state, solver.c:2038, while the gradients stay
+// those of the last residual evaluation): per boundary face, the ghost primitives of the current cell
+// primitives (into dbg_ghost, reference order) and the boundary viscous flux of the current primitives and
+// gradients (into FV).
+// ------------------------------------------------------------------------------------------------
+template <int MODEL>
+__global__ void __launch_bounds__(BLOCK) k_wall_data(const Prm* __restrict__ P, const __grid_constant__ Mesh m,
+                                                     const __grid_constant__ State s)
+{
+    constexpr int NP = Model<MODEL>::NP;
+    const int b = blockIdx.x * BLOCK + threadIdx.x;
+    if (b >= m.nb) return;
+    const int nc = m.nc, c = m.bown[b];
+    const Prm& p = P[cell_solve(s, c)];
+    const int flag = m.bflag[b];
+    const double2 dSv = m.bn[b];
+    const double dSx = dSv.x, dSy = dSv.y, dS = m.bds[b];
+    double E0[NP], G[NP];
+    loadP<MODEL>(s, nc, c, E0);
+    ghost_state<MODEL>(p, flag, dSx, dSy, dS, E0, m.wall_d ? m.wall_d[c] : 0.0, G);
+    const int bo = m.bold[b];
+#pragma unroll
+    for (int k = 0; k < NP; k++) s.dbg_ghost[(size_t)bo * NP + k] = G[k];
+    if (p.visc) {
+        double gvx[5], gvy[5];
+        owner_visc_gradients<MODEL>(s, nc, c, gvx, gvy);
+        bface_visc<MODEL>(p, m, s, b, m.nf + b, c, flag, dSx, dSy, E0, gvx, gvy, m.bd[b], m.bL[b]);
+    }
+}
+
 // ------------------------------------------------------------------------------------------------
 // k_flux: interior faces (blocks [0, nbi)) and boundary faces (blocks [nbi, ...)).
 // coef: also record the wall pressure-coefficient terms of solverCalcCoeff3 (solver.c:1360-1385).
@@ -607,39 +689,10 @@ __global__ void __launch_bounds__(FB) k_flux(const Prm* __restrict__ P, const __
         double2 bdv = make_double2(0.0, 0.0);
         double bLv = 0.0;
         if (p.visc) {
-            double4 a = s.G4x[c], bb = s.G4y[c];
-            gvx[0] = a.y; gvx[1] = a.z; gvx[2] = s.GTx[c];
-            gvy[0] = bb.y; gvy[1] = bb.z; gvy[2] = s.GTy[c];
-            gvx[3] = MODEL >= 1 ? s.Gxx[c] : 0.0;
-            gvy[3] = MODEL >= 1 ? s.Gxy[c] : 0.0;
-            gvx[4] = MODEL == 2 ? s.Gxx[(size_t)nc + c] : (MODEL == 1 ? a.x : 0.0); // SA: the rho gradient (saCC)
-            gvy[4] = MODEL == 2 ? s.Gxy[(size_t)nc + c] : (MODEL == 1 ? bb.x : 0.0);
+            owner_visc_gradients<MODEL>(s, nc, c, gvx, gvy);
             bdv = m.bd[b];
             bLv = m.bL[b];
-        }
-        if constexpr (MODEL == 2) {
-            double2 un = m.bun[b];
-            double fv[5];
-            sst_boundary_flux(p.gas, p.sst_k, p.pr, p.pr_t, p.t_wall, p.pin, flag, gvx, gvy, E0, m.wall_d[c], dSx,
-                              dSy, bdv.x, bdv.y, bLv, un.x, un.y, m.bds2[b], fv);
-            s.FV[fi] = make_double4(fv[0], fv[1], fv[2], fv[3]);
-            s.FV5[fi] = fv[4];
-        } else if constexpr (MODEL == 1) {
-            double2 un = m.bun[b];
-            double fv[4];
-            if (p.sa_cc)
-                sacc_boundary_flux(p.gas, p.pr, p.pr_t, p.t_wall, p.pin, flag, gvx, gvy, E0, dSx, dSy, bdv.x, bdv.y,
-                                   bLv, un.x, un.y, m.bds2[b], fv);
-            else
-                sa_boundary_flux(p.gas, p.pr, p.pr_t, p.t_wall, p.pin, flag, gvx, gvy, E0, dSx, dSy, bdv.x, bdv.y, bLv,
-                                 un.x, un.y, m.bds2[b], fv);
-            s.FV[fi] = make_double4(fv[0], fv[1], fv[2], fv[3]);
-        } else if (p.laminar == 1) {
-            double2 un = m.bun[b];
-            double fv[3];
-            laminar_boundary(p.gas, p.pr, p.t_wall, p.pin, flag, gvx, gvy, E0, dSx, dSy, bdv.x, bdv.y, bLv, un.x,
-                             un.y, m.bds2[b], fv);
-            s.FV[fi] = make_double4(fv[0], fv[1], fv[2], 0.0);
+            bface_visc<MODEL>(p, m, s, b, fi, c, flag, dSx, dSy, E0, gvx, gvy, bdv, bLv);
         }
         if (coef && (flag == 3 || flag == 4)) {
             double G[NP];
@@ -1415,15 +1468,35 @@ __global__ void __launch_bounds__(BLOCK) k_finalize(const Prm* __restrict__ P, c
 #pragma unroll
     for (int k = 0; k < NV + 4; k++) v[k] = 0.0;
     if (mode != 2) {
-        // contiguous chunks per thread, then a fixed tree: deterministic
-        int per = (npart + BLOCK - 1) / BLOCK;
-        for (int i = threadIdx.x * per; i < min(npart, (int)(threadIdx.x + 1) * per); i++)
+        // rows strided over the threads (consecutive threads read consecutive rows), four rows per thread in
+        // flight before any is added, then a fixed tree: deterministic
+        constexpr int U = 4;
+        for (int i0 = threadIdx.x; i0 < npart; i0 += U * BLOCK) {
+            double t[U][NV];
 #pragma unroll
-            for (int k = 0; k < NV; k++) v[k] += part[(size_t)i * NV + k];
-        int perw = (nwall + BLOCK - 1) / BLOCK;
-        for (int i = threadIdx.x * perw; i < min(nwall, (int)(threadIdx.x + 1) * perw); i++)
+            for (int u = 0; u < U; u++) {
+                const int i = i0 + u * BLOCK;
 #pragma unroll
-            for (int k = 0; k < 4; k++) v[NV + k] += bcoef[(size_t)i * 4 + k];
+                for (int k = 0; k < NV; k++) t[u][k] = i < npart ? part[(size_t)i * NV + k] : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++)
+#pragma unroll
+                for (int k = 0; k < NV; k++) v[k] += t[u][k];
+        }
+        for (int i0 = threadIdx.x; i0 < nwall; i0 += U * BLOCK) {
+            double t[U][4];
+#pragma unroll
+            for (int u = 0; u < U; u++) {
+                const int i = i0 + u * BLOCK;
+#pragma unroll
+                for (int k = 0; k < 4; k++) t[u][k] = i < nwall ? bcoef[(size_t)i * 4 + k] : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < U; u++)
+#pragma unroll
+                for (int k = 0; k < 4; k++) v[NV + k] += t[u][k];
+        }
     }
     Scalars S;
     if (threadIdx.x == 0) S = *sc;

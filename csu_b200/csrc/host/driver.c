@@ -12,11 +12,13 @@
  *                    saCC.c:599-745, sst.c:820-962; dispatched as solverWriteSurf, solver.c:1984-2007)
  *
  * The iteration history comes from the device (csu_iterate). Node interpolation and file writing stay on
- * the host: they run once per solve. friction.csv and surfData.csv are written, as in the reference, from
- * what the last iteration's residual evaluation left: primitives, ghost states and gradients of the state
- * that iteration started from (the reference never recomputes them after its last update). The engine
- * therefore runs Nmax - 1 iterations, evaluates the residual of that state once (csu_residual: it leaves
- * exactly those arrays on the device), writes the two files, and runs the last iteration.
+ * the host: they run once per solve. The wall files follow the reference's order of events. friction.csv is
+ * written inside solverSolve from what the last iteration's residual evaluation left: primitives and
+ * gradients of the state that iteration started from. The engine therefore runs Nmax - 1 iterations,
+ * evaluates the residual of that state once (csu_residual leaves exactly those arrays on the device), writes
+ * friction.csv, and runs the last iteration. surfData.csv comes after solverWriteSolution2, which recomputes
+ * the cell and ghost primitives of the final state: csu_wall_data gives the ghost states and boundary
+ * viscous fluxes of the final primitives with the last gradients.
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -415,18 +417,11 @@ int csu_run_case(const char* wd, int verbose)
             if (visc && it + n == nmax) {
                 if (n > 1) n--;
                 else {
-                    /* the last iteration: first the wall files from the state it starts from */
-                    double *GP = malloc(sizeof(double) * (size_t)(nv + 1) * (d.n_bfaces > 0 ? d.n_bfaces : 1));
-                    double *BV = malloc(sizeof(double) * (size_t)4 * (d.n_bfaces > 0 ? d.n_bfaces : 1));
+                    /* the last iteration: first friction.csv from the state it starts from */
                     st = csu_residual(ctx, NULL);
                     if (!st) st = csu_dump(ctx, CSU_DUMP_GRAD, G);
                     if (!st) st = csu_dump(ctx, CSU_DUMP_P, P);
-                    if (!st) st = csu_dump(ctx, CSU_DUMP_GHOST_P, GP);
-                    if (!st) st = csu_dump(ctx, CSU_DUMP_BVISC, BV);
                     if (!st) st = write_friction(wd, cs, P, G);
-                    if (!st) st = write_surf(wd, cs, GP, BV, P);
-                    free(GP);
-                    free(BV);
                     if (st) goto done;
                     wrote_wall = 1;
                 }
@@ -460,6 +455,19 @@ int csu_run_case(const char* wd, int verbose)
         if (verbose) printf("\nmain: running solution:\n");
         if ((st = csu_tube_run(ctx, tmax, &steps, &t))) goto done;
         if (verbose) printf("time %f s\n", t);
+    }
+    if (wrote_wall) {
+        /* surfData.csv: the final state's primitives and ghost states, the last gradients */
+        double* GP = malloc(sizeof(double) * (size_t)(nv + 1) * (d.n_bfaces > 0 ? d.n_bfaces : 1));
+        double* BV = malloc(sizeof(double) * (size_t)4 * (d.n_bfaces > 0 ? d.n_bfaces : 1));
+        st = csu_wall_data(ctx);
+        if (!st) st = csu_dump(ctx, CSU_DUMP_GHOST_P, GP);
+        if (!st) st = csu_dump(ctx, CSU_DUMP_BVISC, BV);
+        if (!st) st = csu_dump(ctx, CSU_DUMP_P, P);
+        if (!st) st = write_surf(wd, cs, GP, BV, P);
+        free(GP);
+        free(BV);
+        if (st) goto done;
     }
     if ((st = csu_get_state(ctx, U))) goto done;
     if ((st = write_solution(wd, cs, U))) goto done;

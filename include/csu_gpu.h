@@ -211,6 +211,12 @@ int csu_tube_run(csu_ctx* ctx, double tmax, int* steps, double* t_final);
 #define CSU_DUMP_BVISC 13
 int csu_dump(csu_ctx* ctx, int what, double* out);
 
+/* Ghost primitives and boundary viscous fluxes of the current state, the inputs of the reference's surface
+ * writers after its last iteration (laminar.c:350-492, sa.c:854-996, sst.c:820-962): solverWriteSolution2
+ * recomputes the cell and ghost primitives of the final state (solver.c:2038) while the gradients stay those
+ * of the last residual evaluation. Afterwards CSU_DUMP_GHOST_P and CSU_DUMP_BVISC return them. */
+int csu_wall_data(csu_ctx* ctx);
+
 /* Run the engine's work on a caller-provided cudaStream_t (NULL: the context's own stream). */
 int csu_set_stream(csu_ctx* ctx, void* stream);
 
