@@ -93,6 +93,8 @@ def lib():
         L.csu_tube_run.argtypes = [vp, C.c_double, ip, dp]
         L.csu_dump.argtypes = [vp, C.c_int, vp]
         L.csu_wall_data.argtypes = [vp]
+        L.csu_autotune.argtypes = [vp, ip, ip]
+        L.csu_iterate_views.argtypes = [vp, C.c_int, vp, vp, vp]
         L.csu_stats.argtypes = [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
         L.csu_set_stream.argtypes = [vp, vp]
         L.csu_time_kernels.argtypes = [vp, C.c_int, dp, ip]
@@ -302,6 +304,13 @@ class Engine:
         a, b = C.c_longlong(), C.c_longlong()
         _check(lib().csu_stats(self._h, C.byref(a), C.byref(b)))
         return {"kernel_launches": a.value, "device_bytes": b.value}
+
+    def autotune(self):
+        """Times the launch shapes on this solve and keeps the fastest: (faces per flux block, cells per
+        sweep block)."""
+        fb, sb = C.c_int(), C.c_int()
+        _check(lib().csu_autotune(self._h, C.byref(fb), C.byref(sb)))
+        return fb.value, sb.value
 
     def close(self):
         if getattr(self, "_h", None) and _lib is not None:

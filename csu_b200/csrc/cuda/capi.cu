@@ -8,6 +8,8 @@
 #include <vector>
 #include <algorithm>
 #include <mutex>
+#include <map>
+#include <tuple>
 #include "csu_gpu.h"
 #include "kernels.cuh"
 
@@ -87,11 +89,11 @@ const double RK5[5] = {0.0533, 0.1263, 0.2375, 0.4414, 1.0};
 
 } // namespace
 
-// DPLUR sweeps run in blocks of SWEEP_BLOCK threads (more resident blocks per SM, finer waves); the first
-// sweep's partial norms then come one row per SWEEP_BLOCK cells.
-#ifndef SWEEP_BLOCK
-#define SWEEP_BLOCK 128
-#endif
+// Launch shapes the autotuner chooses among (csu_autotune): faces per k_flux block and cells per DPLUR sweep
+// block. Neither changes a result bit: fluxes are per face, sweeps per cell, and the first sweep's partial
+// norms come one row per warp whatever the block size.
+static const int FLUX_BLOCKS[3] = {32, 64, 128};
+static const int SWEEP_BLOCKS[3] = {64, 128, 256};
 
 struct csu_ctx {
     int model = 0, nv = 4;
@@ -127,6 +129,8 @@ struct csu_ctx {
     long long graph_launches[4][2] = {};
     Scalars* h_sc = nullptr;   // pinned: solve 0's scalars, read back once at the end of csu_iterate
     int* h_flags = nullptr;    // pinned: halt flags (status, done) of two chunks in flight
+    bool snap = false;         // csu_iterate_views: copy the last residual evaluation's primitives/gradients
+    double* h_snap = nullptr;  // pinned: those copies (W4, WT, Wx, G4x, G4y, Gxx, Gxy in device order)
     cudaEvent_t ev_poll[2] = {nullptr, nullptr};
     double* h_hist = nullptr;  // pinned: solve 0's history rows (hist_cap rows)
     int have_debug = 0;
@@ -135,6 +139,9 @@ struct csu_ctx {
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int max_ni = 4;          // most interior faces of a cell (k_blocks covers slots [0, max_ni))
+    int flux_fb = 64;        // faces per k_flux block (one of FLUX_BLOCKS)
+    int sweep_sb = 128;      // cells per DPLUR sweep block (one of SWEEP_BLOCKS)
+    bool tuned = false;      // launch shapes chosen (csu_autotune, or its cache on the first iteration)
     int device = 0;          // the CUDA device current when the context was made (its memory lives there)
     int sm_count = 148;      // that device's multiprocessors
     // one-solve contexts: the renumbering on the device and a staging buffer for the state in reference order
@@ -285,7 +292,7 @@ static void plan(csu_ctx* x, Arena& a)
     s.blocks = dplur && !x->cfg.implicit_fp32 ? carve<double>(a, c4 * nv * nv) : nullptr;
     s.blocks32 = dplur && x->cfg.implicit_fp32 ? carve<float>(a, c4 * nv * nv) : nullptr;
     // partial norms: one row per 256-cell block, or per 128-cell block from the DPLUR first sweep
-    s.part = carve<double>(a, (size_t)((nc + BLOCK - 1) / BLOCK) * (BLOCK / SWEEP_BLOCK) * nv);
+    s.part = carve<double>(a, (size_t)((nc + BLOCK - 1) / BLOCK) * (BLOCK / 32) * nv);
     s.bcoef = carve<double>(a, (size_t)4 * (nb > 0 ? nb : 1));
     s.sc = carve<Scalars>(a, x->nsolve);
     s.bsolve = x->nsolve > 1 ? carve<int>(a, (nc + BLOCK - 1) / BLOCK) : nullptr;
@@ -696,6 +703,7 @@ extern "C" void csu_destroy(csu_ctx* x)
     if (x->h_sc) cudaFreeHost(x->h_sc);
     if (x->h_hist) cudaFreeHost(x->h_hist);
     if (x->h_flags) cudaFreeHost(x->h_flags);
+    if (x->h_snap) cudaFreeHost(x->h_snap);
     for (cudaEvent_t e : x->ev_poll)
         if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : x->ev) cudaEventDestroy(e);
@@ -884,16 +892,22 @@ static void launch_grad(csu_ctx* x, bool dbg)
     tmark(x, KGRAD);
 }
 
-// faces in blocks of FLUX_BLOCK threads (more resident blocks per SM, finer waves)
-#ifndef FLUX_BLOCK
-#define FLUX_BLOCK 64
-#endif
+// faces in blocks of FB threads
+template <int MODEL, int FB>
+static void launch_flux_fb(csu_ctx* x, int coef)
+{
+    const int gi = (x->L.nf + FB - 1) / FB, gb = (x->L.nb + FB - 1) / FB;
+    k_flux<MODEL, FB><<<gi + gb, FB, 0, x->stream>>>(x->d_prm, x->mesh, x->st, gi, x->d_wall_rank, coef);
+}
+
 template <int MODEL>
 static void launch_flux(csu_ctx* x, int coef)
 {
-    constexpr int FB = FLUX_BLOCK;
-    const int gi = (x->L.nf + FB - 1) / FB, gb = (x->L.nb + FB - 1) / FB;
-    k_flux<MODEL, FB><<<gi + gb, FB, 0, x->stream>>>(x->d_prm, x->mesh, x->st, gi, x->d_wall_rank, coef);
+    switch (x->flux_fb) {
+    case 32: launch_flux_fb<MODEL, 32>(x, coef); break;
+    case 128: launch_flux_fb<MODEL, 128>(x, coef); break;
+    default: launch_flux_fb<MODEL, 64>(x, coef); break;
+    }
     x->launches++;
     tmark(x, KFLUX);
 }
@@ -901,7 +915,8 @@ static void launch_flux(csu_ctx* x, int coef)
 template <int MODEL>
 static void launch_finalize(csu_ctx* x, int mode)
 {
-    const int ppb = x->cfg.time_scheme == CSU_TS_DPLUR && mode == 1 ? BLOCK / SWEEP_BLOCK : 1;
+    // the first DPLUR sweep writes one partial row per warp; the other kernels one per cell block
+    const int ppb = x->cfg.time_scheme == CSU_TS_DPLUR && mode == 1 ? BLOCK / 32 : 1;
     k_finalize<MODEL><<<x->nsolve, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st, mode, ppb);
     x->launches++;
     tmark(x, KFIN);
@@ -939,10 +954,9 @@ static void launch_blocks(csu_ctx* x)
     else cudaEventRecord(x->ev_join, x->side);
 }
 
-template <int MODEL>
-static void launch_sweep(csu_ctx* x, int m, int n)
+template <int MODEL, int SB>
+static void launch_sweep_sb(csu_ctx* x, int m, int n)
 {
-    constexpr int SB = SWEEP_BLOCK;
     if (m == 0) {
         auto* k = m == n - 1 ? k_sweep<MODEL, true, true, SB> : k_sweep<MODEL, false, true, SB>;
         k<<<x->gb_c * (BLOCK / SB), SB, 0, x->stream>>>(x->d_prm, x->mesh, x->st, m, x->xcur);
@@ -950,9 +964,39 @@ static void launch_sweep(csu_ctx* x, int m, int n)
         auto* k = m == n - 1 ? k_sweep<MODEL, true, false, SB> : k_sweep<MODEL, false, false, SB>;
         k<<<x->gb_c * (BLOCK / SB), SB, 0, x->stream>>>(x->d_prm, x->mesh, x->st, m, x->xcur);
     }
+}
+
+template <int MODEL>
+static void launch_sweep(csu_ctx* x, int m, int n)
+{
+    switch (x->sweep_sb) {
+    case 64: launch_sweep_sb<MODEL, 64>(x, m, n); break;
+    case 256: launch_sweep_sb<MODEL, 256>(x, m, n); break;
+    default: launch_sweep_sb<MODEL, 128>(x, m, n); break;
+    }
     x->launches++;
     tmark(x, KSWEEP);
     x->xcur ^= 1;
+}
+
+// csu_iterate_views: the primitives and gradients the residual evaluation just launched works on, copied in
+// stream order to pinned host memory (device layout; unpacked after the iteration)
+static void snapshot_views(csu_ctx* x)
+{
+    if (!x->snap || !x->h_snap) return;
+    const size_t nc = x->L.nc, nx = x->nv - 4;
+    double* h = x->h_snap;
+    auto cp = [&](const void* src, size_t n) {
+        if (n) cudaMemcpyAsync(h, src, sizeof(double) * n, cudaMemcpyDeviceToHost, x->stream);
+        h += n;
+    };
+    cp(x->st.W4, 4 * nc);
+    cp(x->st.WT, nc);
+    cp(x->st.Wx, nx * nc);
+    cp(x->st.G4x, 4 * nc);
+    cp(x->st.G4y, 4 * nc);
+    cp(x->st.Gxx, nx * nc);
+    cp(x->st.Gxy, nx * nc);
 }
 
 // one iteration of the steady loop body (solver.c:1866-1906)
@@ -964,6 +1008,7 @@ static void launch_iteration(csu_ctx* x)
         for (int sgi = 0; sgi < c.stages; sgi++) {
             bool last = sgi == c.stages - 1;
             if (c.order == 2 || x->prm.visc) launch_grad<MODEL>(x, false);
+            if (last) snapshot_views(x);
             launch_flux<MODEL>(x, last ? 1 : 0);
             if (last) k_rk<MODEL, true><<<x->gb_c, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st, x->rk[sgi]);
             else k_rk<MODEL, false><<<x->gb_c, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st, x->rk[sgi]);
@@ -973,6 +1018,7 @@ static void launch_iteration(csu_ctx* x)
         launch_finalize<MODEL>(x, 0);
     } else if (c.time_scheme == CSU_TS_LUSGS) {
         if (c.order == 2 || x->prm.visc) launch_grad<MODEL>(x, false);
+        snapshot_views(x);
         launch_flux<MODEL>(x, 1);
         k_impl<MODEL, true><<<x->gb_c, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st);
         x->launches++;
@@ -1004,6 +1050,7 @@ static void launch_iteration(csu_ctx* x)
         const bool grad = c.order == 2 || x->prm.visc;
         if (!x->timing) cudaEventRecord(x->ev_fork, x->stream);
         if (grad) launch_grad<MODEL>(x, false);
+        snapshot_views(x);
         if (early) launch_blocks<MODEL>(x);
         launch_flux<MODEL>(x, 1);
         if (!early) {
@@ -1093,6 +1140,163 @@ static int build_graph(csu_ctx* x, int gi)
     return CSU_OK;
 }
 
+// ------------------------------------------------------------------------------------------------ autotuner
+// Launch shapes of k_flux (faces per block) and of the DPLUR sweeps (cells per block) picked by timing each
+// candidate on the context itself: `reps` launches after one warm-up, CUDA events on the context's stream.
+// The timed launches leave no trace a later iteration could see: k_flux rewrites the face fluxes the next
+// iteration computes again before reading them; the timed sweep is a middle sweep that writes the spare
+// increment buffer (the next iteration's first sweep overwrites it) and uses the last early-exit slot pair,
+// cleared afterwards. Choices are cached per device, model, order, viscosity, block precision and size class
+// (half octaves of the cell count), so packs of a size class seen before take the cached shapes.
+namespace {
+struct TuneKey {
+    int dev, model, order, visc, blk32, implicit, size_class;
+    bool operator<(const TuneKey& o) const
+    {
+        return std::tie(dev, model, order, visc, blk32, implicit, size_class) <
+               std::tie(o.dev, o.model, o.order, o.visc, o.blk32, o.implicit, o.size_class);
+    }
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, std::pair<int, int>> g_tune_cache;
+} // namespace
+
+template <int MODEL>
+static int time_flux_shape(csu_ctx* x, int fb, int reps, cudaEvent_t e0, cudaEvent_t e1, float* ms)
+{
+    const int save = x->flux_fb;
+    x->flux_fb = fb;
+    const long long l0 = x->launches;
+    launch_flux<MODEL>(x, 1);
+    CK(cudaEventRecord(e0, x->stream));
+    for (int r = 0; r < reps; r++) launch_flux<MODEL>(x, 1);
+    CK(cudaEventRecord(e1, x->stream));
+    x->flux_fb = save;
+    x->launches = l0;
+    CK(cudaGetLastError());
+    CK(cudaEventSynchronize(e1));
+    CK(cudaEventElapsedTime(ms, e0, e1));
+    return CSU_OK;
+}
+
+template <int MODEL>
+static int time_sweep_shape(csu_ctx* x, int sb, int reps, cudaEvent_t e0, cudaEvent_t e1, float* ms)
+{
+    // the slot before the timed one says "not converged" so the timed sweep does its full work
+    const int slot = MAX_SWEEPS - 1;
+    std::vector<unsigned long long> big(x->nsolve, 0x3ff0000000000000ULL); // 1.0 for every solve
+    CK(cudaMemcpy2DAsync(&x->st.sc[0].sweep_max[slot - 1], sizeof(Scalars), big.data(), sizeof(unsigned long long),
+                         sizeof(unsigned long long), x->nsolve, cudaMemcpyHostToDevice, x->stream));
+    auto launch = [&]() {
+        switch (sb) {
+        case 64: k_sweep<MODEL, false, false, 64><<<x->gb_c * (BLOCK / 64), 64, 0, x->stream>>>(x->d_prm, x->mesh, x->st, slot, x->xcur); break;
+        case 256: k_sweep<MODEL, false, false, 256><<<x->gb_c, 256, 0, x->stream>>>(x->d_prm, x->mesh, x->st, slot, x->xcur); break;
+        default: k_sweep<MODEL, false, false, 128><<<x->gb_c * 2, 128, 0, x->stream>>>(x->d_prm, x->mesh, x->st, slot, x->xcur); break;
+        }
+    };
+    launch();
+    CK(cudaEventRecord(e0, x->stream));
+    for (int r = 0; r < reps; r++) launch();
+    CK(cudaEventRecord(e1, x->stream));
+    CK(cudaGetLastError());
+    CK(cudaMemset2DAsync(&x->st.sc[0].sweep_max[slot - 1], sizeof(Scalars), 0, 2 * sizeof(unsigned long long),
+                         x->nsolve, x->stream));
+    CK(cudaEventSynchronize(e1));
+    CK(cudaEventElapsedTime(ms, e0, e1));
+    return CSU_OK;
+}
+
+template <int MODEL>
+static int tune_shapes(csu_ctx* x, int* fb_out, int* sb_out)
+{
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    cudaError_t e = cudaEventCreate(&e1);
+    if (e != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return cuda_fail(e, "cudaEventCreate");
+    }
+    const int reps = 5;
+    int st = CSU_OK;
+    float best = 1e30f;
+    *fb_out = x->flux_fb;
+    for (int fb : FLUX_BLOCKS) {
+        float ms = 0;
+        if ((st = time_flux_shape<MODEL>(x, fb, reps, e0, e1, &ms))) break;
+        if (ms < best) {
+            best = ms;
+            *fb_out = fb;
+        }
+    }
+    *sb_out = x->sweep_sb;
+    if (!st && x->cfg.time_scheme == CSU_TS_DPLUR) {
+        best = 1e30f;
+        for (int sb : SWEEP_BLOCKS) {
+            float ms = 0;
+            if ((st = time_sweep_shape<MODEL>(x, sb, reps, e0, e1, &ms))) break;
+            if (ms < best) {
+                best = ms;
+                *sb_out = sb;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return st;
+}
+
+// Picks the launch shapes of x (from the cache, or by timing when its class has not been seen); contexts
+// under 16,384 cells keep the defaults (launch latency, not the shape, bounds them). CSU_AUTOTUNE=0 keeps
+// the defaults everywhere.
+static int autotune(csu_ctx* x, bool force)
+{
+    if (x->tuned && !force) return CSU_OK;
+    x->tuned = true;
+    const char* env = getenv("CSU_AUTOTUNE");
+    if (env && strcmp(env, "0") == 0) return CSU_OK;
+    if (x->L.nc < 16384 && !force) return CSU_OK;
+    TuneKey key{x->device, x->model, x->cfg.order, x->prm.visc, x->cfg.implicit_fp32,
+                x->cfg.time_scheme, (int)floor(2.0 * log2((double)x->L.nc))};
+    int fb = x->flux_fb, sb = x->sweep_sb;
+    bool hit = false;
+    if (!force) {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) {
+            fb = it->second.first;
+            sb = it->second.second;
+            hit = true;
+        }
+    }
+    if (!hit) {
+        int st;
+        switch (x->model) {
+        case 0: st = tune_shapes<0>(x, &fb, &sb); break;
+        case 1: st = tune_shapes<1>(x, &fb, &sb); break;
+        default: st = tune_shapes<2>(x, &fb, &sb); break;
+        }
+        if (st) return st;
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune_cache[key] = {fb, sb};
+    }
+    if (fb != x->flux_fb || sb != x->sweep_sb) {
+        x->flux_fb = fb;
+        x->sweep_sb = sb;
+        drop_graphs(x);
+    }
+    return CSU_OK;
+}
+
+extern "C" int csu_autotune(csu_ctx* x, int* flux_faces_per_block, int* sweep_cells_per_block)
+{
+    if (!x) return CSU_ERR_INPUT;
+    int st = autotune(x, true);
+    if (st) return st;
+    if (flux_faces_per_block) *flux_faces_per_block = x->flux_fb;
+    if (sweep_cells_per_block) *sweep_cells_per_block = x->sweep_sb;
+    return CSU_OK;
+}
+
 // Start of a call on the device: history rows and the call's iteration count restart; a one-solve context
 // also restarts its loop counter at it0 (the solves of a pack keep their own).
 __global__ void k_call_begin(Scalars* sc, int n, int it0, int set_iter)
@@ -1131,6 +1335,7 @@ static int run_iterations(csu_ctx* x, int n, int it0, Scalars* out, double* hist
         if ((st = check_launch("prologue"))) return st;
         x->prepared = 1;
     }
+    if ((st = autotune(x, false))) return st;
     if (!x->is_pack) {
         // every size at the parities this context can start a graph with
         for (int gi = 0; gi < 4; gi++)
@@ -1212,6 +1417,61 @@ extern "C" int csu_iterate_ex(csu_ctx* x, int n, int it0, double* hist, int* n_d
 extern "C" int csu_iterate(csu_ctx* x, int n, int it0, double* hist)
 {
     return csu_iterate_ex(x, n, it0, hist, nullptr);
+}
+
+extern "C" int csu_iterate_views(csu_ctx* x, int it0, double* hist, double* P, double* G)
+{
+    if (!x || !P || !G) return CSU_ERR_INPUT;
+    if (x->is_pack) {
+        csu_set_error("csu_iterate_views: views in reference order are per solve and not available for packs");
+        return CSU_ERR_STATE;
+    }
+    const int nc = x->L.nc, nv = x->nv, nx = nv - 4;
+    if (!x->h_snap) CK(cudaMallocHost((void**)&x->h_snap, sizeof(double) * (size_t)nc * (5 + nx + 8 + 2 * nx)));
+    int st;
+    if ((st = ensure_hist(x, 1))) return st;
+    if (!x->h_sc) CK(cudaMallocHost((void**)&x->h_sc, sizeof(Scalars)));
+    if (!x->prepared) {
+        if ((st = reset_scalars(x, it0))) return st;
+        DISPATCH(launch_prologue, x);
+        x->prepared = 1;
+    } else {
+        k_call_begin<<<1, 32, 0, x->stream>>>(x->st.sc, 1, it0, 1);
+        x->launches++;
+    }
+    if ((st = autotune(x, false))) return st;
+    // one iteration launched directly (not from a graph), copying the views at its last residual evaluation
+    x->snap = true;
+    DISPATCH(launch_iteration, x);
+    x->snap = false;
+    if ((st = check_launch("csu_iterate_views"))) return st;
+    CK(cudaMemcpyAsync(x->h_sc, x->st.sc, sizeof(Scalars), cudaMemcpyDeviceToHost, x->stream));
+    CK(cudaStreamSynchronize(x->stream));
+    const Scalars h = *x->h_sc;
+    if (hist && h.hist_row > 0) CK(cudaMemcpy(hist, x->hist, sizeof(double) * (nv + 4), cudaMemcpyDeviceToHost));
+    const int* n2o = x->L.cell_new2old;
+    const double *W4 = x->h_snap, *WT = W4 + 4 * (size_t)nc, *Wx = WT + nc, *G4x = Wx + (size_t)nx * nc,
+                 *G4y = G4x + 4 * (size_t)nc, *Gxx = G4y + 4 * (size_t)nc, *Gxy = Gxx + (size_t)nx * nc;
+    for (int c = 0; c < nc; c++) {
+        const int o = n2o[c];
+        double* row = P + (size_t)o * (nv + 1);
+        for (int k = 0; k < 4; k++) row[k] = W4[(size_t)4 * c + k];
+        row[4] = WT[c];
+        for (int k = 5; k < nv + 1; k++) row[k] = Wx[(size_t)(k - 5) * nc + c];
+        for (int k = 0; k < 4; k++) {
+            G[(size_t)k * nc + o] = G4x[(size_t)4 * c + k];
+            G[(size_t)(nv + k) * nc + o] = G4y[(size_t)4 * c + k];
+        }
+        for (int k = 4; k < nv; k++) {
+            G[(size_t)k * nc + o] = Gxx[(size_t)(k - 4) * nc + c];
+            G[(size_t)(nv + k) * nc + o] = Gxy[(size_t)(k - 4) * nc + c];
+        }
+    }
+    if (h.status) {
+        csu_set_error("csu_iterate_views: state became non-finite at iteration %d", h.iter);
+        return h.status;
+    }
+    return CSU_OK;
 }
 
 extern "C" int csu_tube_run(csu_ctx* x, double tmax, int* steps, double* t_final)

@@ -829,6 +829,20 @@ __device__ __forceinline__ void partial_norms(const State& s, bool valid, const 
         for (int k = 0; k < NV; k++) s.part[(size_t)blockIdx.x * NV + k] = v[k];
 }
 
+// The same partial sums one row per warp (32 cells, row = cell / 32), whatever the block size of the
+// kernel: the rows, and so the norms summed from them, do not depend on the launch shape.
+template <int MODEL>
+__device__ __forceinline__ void partial_norms_warp(const State& s, bool valid, const double* R, int c)
+{
+    constexpr int NV = Model<MODEL>::NV;
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int k = 0; k < NV; k++) {
+        const double x = warp_sum(valid ? R[k] * R[k] : 0.0);
+        if (lane == 0) s.part[(size_t)(c >> 5) * NV + k] = x;
+    }
+}
+
 // ------------------------------------------------------------------------------------------------
 // k_resid: R only (csu_residual).
 // ------------------------------------------------------------------------------------------------
@@ -1210,7 +1224,7 @@ __global__ void __launch_bounds__(SB) k_sweep(const Prm* __restrict__ P, const _
         double v = block_max<SB>(dmax);
         if (threadIdx.x == 0) atomicMax(&sc->sweep_max[sweep], dbits(v));
     }
-    if (FIRST) partial_norms<MODEL, SB>(s, valid, R);
+    if (FIRST) partial_norms_warp<MODEL>(s, valid, R, c);
 }
 
 // implicitCalcDeltaFlux (implicit.c:194-231) and implicitCalcDeltaFlux_sa (495-552): F(U + d) - F(U) on the

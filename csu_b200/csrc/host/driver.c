@@ -13,10 +13,10 @@
  *
  * The iteration history comes from the device (csu_iterate). Node interpolation and file writing stay on
  * the host: they run once per solve. The wall files follow the reference's order of events. friction.csv is
- * written inside solverSolve from what the last iteration's residual evaluation left: primitives and
- * gradients of the state that iteration started from. The engine therefore runs Nmax - 1 iterations,
- * evaluates the residual of that state once (csu_residual leaves exactly those arrays on the device), writes
- * friction.csv, and runs the last iteration. surfData.csv comes after solverWriteSolution2, which recomputes
+ * written inside solverSolve from what the last residual evaluation left: primitives and gradients of the
+ * state the last iteration started from (implicit schemes) or of its last RK stage's input. The engine
+ * therefore runs Nmax - 1 iterations, then the last one through csu_iterate_views, which returns exactly
+ * those arrays, and writes friction.csv. surfData.csv comes after solverWriteSolution2, which recomputes
  * the cell and ghost primitives of the final state: csu_wall_data gives the ghost states and boundary
  * viscous fluxes of the final primitives with the last gradients.
  */
@@ -417,16 +417,13 @@ int csu_run_case(const char* wd, int verbose)
             if (visc && it + n == nmax) {
                 if (n > 1) n--;
                 else {
-                    /* the last iteration: first friction.csv from the state it starts from */
-                    st = csu_residual(ctx, NULL);
-                    if (!st) st = csu_dump(ctx, CSU_DUMP_GRAD, G);
-                    if (!st) st = csu_dump(ctx, CSU_DUMP_P, P);
-                    if (!st) st = write_friction(wd, cs, P, G);
-                    if (st) goto done;
+                    /* the last iteration, with the views of its last residual evaluation for friction.csv */
+                    if ((st = csu_iterate_views(ctx, it, hist, P, G))) goto done;
+                    if ((st = write_friction(wd, cs, P, G))) goto done;
                     wrote_wall = 1;
                 }
             }
-            if ((st = csu_iterate(ctx, n, it, hist))) goto done;
+            if (!wrote_wall && (st = csu_iterate(ctx, n, it, hist))) goto done;
             for (int r = 0; r < n; r++) {
                 const double* h = hist + (size_t)r * (nv + 4);
                 if (verbose) {

@@ -173,6 +173,13 @@ int csu_iterate(csu_ctx* ctx, int n, int it0, double* hist);
 /* Same, also reporting how many iterations ran before the convergence stop (conv_drop) triggered. */
 int csu_iterate_ex(csu_ctx* ctx, int n, int it0, double* hist, int* n_done);
 
+/* One iteration like csu_iterate(ctx, 1, it0, hist) that also returns what its last residual evaluation
+ * worked on: the cell primitives P (ncells*(nvar+1), [cell][k], as CSU_DUMP_P) and the gradients G (dPx rows
+ * then dPy rows, as CSU_DUMP_GRAD) -- the state the iteration started from for the implicit schemes, the last
+ * stage's input for RK. These are the E->P and dPx the reference's friction output reads after its loop
+ * (solverCalcCoeff2, solver.c:1303-1340, called at 1908). */
+int csu_iterate_views(csu_ctx* ctx, int it0, double* hist, double* P, double* G);
+
 /* The unsteady tube loop (solver.c:1912-1942) up to tmax; returns steps taken and final time. */
 int csu_tube_run(csu_ctx* ctx, double tmax, int* steps, double* t_final);
 
@@ -247,6 +254,14 @@ int csu_time_kernels(csu_ctx* ctx, int iters, double* ms, int* count);
  * overlap on one GPU share the scratch and race. A CUDA error already pending from earlier work is returned
  * (CSU_ERR_CUDA) before anything is launched. */
 int csu_residual_norms_noalloc(const double* R, int nvar, int ncells, double* res, void* stream);
+
+/* Launch-shape autotuner (no counterpart in the reference): times the face-chunk size of the face-flux
+ * kernel (32, 64 or 128 faces per block) and the cell-block size of the DPLUR sweeps (64, 128 or 256) on this
+ * context and keeps the fastest; neither choice changes a result bit. A context tunes itself on its first
+ * csu_iterate (16,384 cells or more; a cache per device, model and size class spares packs of a class seen
+ * before the timing); this call re-times now and reports the choice. CSU_AUTOTUNE=0 in the environment
+ * keeps the default shapes (64 faces, 128 cells). */
+int csu_autotune(csu_ctx* ctx, int* flux_faces_per_block, int* sweep_cells_per_block);
 
 /* Counters of the engine: kernels launched since creation, device bytes held. */
 int csu_stats(csu_ctx* ctx, long long* kernel_launches, long long* device_bytes);
