@@ -120,6 +120,7 @@ def lib():
         L.csu_srv_info.argtypes = [vp, C.c_longlong, C.POINTER(SrvInfo)]
         L.csu_srv_take.argtypes = [vp, C.c_longlong, vp]
         L.csu_srv_cancel.argtypes = [vp, C.c_longlong]
+        L.csu_srv_poll.argtypes = [vp, C.POINTER(C.c_longlong), C.c_int, ip]
         L.csu_srv_message.argtypes = [vp, C.c_longlong, C.c_char_p, C.c_int]
         L.csu_pack_stop.argtypes = [vp, C.c_int]
         L.csu_srv_totals.argtypes = [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
@@ -142,7 +143,8 @@ class SrvConfig(C.Structure):
 
 class SrvInfo(C.Structure):
     _fields_ = [("state", C.c_int), ("iters", C.c_int), ("n_cells", C.c_int), ("drop", C.c_double),
-                ("t_submit", C.c_double), ("t_start", C.c_double), ("t_end", C.c_double), ("status", C.c_int)]
+                ("t_submit", C.c_double), ("t_start", C.c_double), ("t_end", C.c_double), ("status", C.c_int),
+                ("coef", C.c_double * 4)]
 
 
 SRV_STATES = {0: "queued", 1: "running", 2: "converged", 3: "failed", 4: "maxiter", 5: "cancelled"}
@@ -455,7 +457,15 @@ class Server:
         i = SrvInfo()
         _check(lib().csu_srv_info(self._h, rid, C.byref(i)))
         return {"state": SRV_STATES[i.state], "iters": i.iters, "n_cells": i.n_cells, "drop": i.drop,
-                "t_submit": i.t_submit, "t_start": i.t_start, "t_end": i.t_end, "status": i.status}
+                "t_submit": i.t_submit, "t_start": i.t_start, "t_end": i.t_end, "status": i.status,
+                "coef": list(i.coef)}
+
+    def poll(self, cap=4096):
+        """Ids of the requests that reached a final state since the last poll, in that order."""
+        buf = (C.c_longlong * cap)()
+        n = C.c_int()
+        _check(lib().csu_srv_poll(self._h, buf, cap, C.byref(n)))
+        return list(buf[:n.value])
 
     def cancel(self, rid):
         _check(lib().csu_srv_cancel(self._h, rid))

@@ -1384,6 +1384,13 @@ static int run_iterations(csu_ctx* x, int n, int it0, Scalars* out, double* hist
         }
     }
     if ((st = check_launch("iteration"))) return st;
+    if (x->is_pack) {
+        // a pack's results are read per solve (csu_pack_info / csu_pack_infos, which wait for this work), so
+        // the call returns as soon as the iterations are queued and the caller's bookkeeping overlaps them
+        memset(out, 0, sizeof(*out));
+        out->steps = n;
+        return CSU_OK;
+    }
     CK(cudaMemcpyAsync(x->h_sc, x->st.sc, sizeof(Scalars), cudaMemcpyDeviceToHost, x->stream));
     if (hist_rows && x->h_hist)
         CK(cudaMemcpyAsync(x->h_hist, x->hist, sizeof(double) * (size_t)n * (x->nv + 4), cudaMemcpyDeviceToHost,
@@ -2281,6 +2288,8 @@ static int pack_build(const char* who, const csu_prep* const* solves, int n, csu
         csu_set_error("%s: no CUDA device", who);
         return CSU_ERR_NO_DEVICE;
     }
+    // a pack's iterations return without waiting: the old pack's work must be done before it is read
+    if (old) CK(cudaStreamSynchronize(old->stream));
     csu_ctx* x = new csu_ctx();
     x->model = solves[0]->model;
     x->nv = solves[0]->nv;

@@ -92,6 +92,7 @@ struct Req {
     double t_submit = 0, t_start = 0, t_end = 0;
     int iters = 0;
     double drop = 0;
+    double coef[4] = {0, 0, 0, 0};  // force coefficients of its last iteration
     long long bytes = 0;
     Group* group = nullptr;   // the group whose pack holds it (frozen there once finished)
     bool taken = false;       // result taken while still frozen in a pack: freed at the rebuild
@@ -123,6 +124,7 @@ struct csu_srv {
     csu_srv_config cfg;
     std::map<long long, Req*> reqs;
     std::deque<Req*> queue;
+    std::deque<long long> finished;  // ids that reached a final state, not yet polled
     std::vector<Group*> groups;
     long long used = 0;
     long long next_id = 1;
@@ -264,6 +266,7 @@ static int retire(csu_srv* s, Group* g)
         const csu_solve_info& info = infos[k];
         r->iters = info.iter;
         r->drop = info.have_res0 && info.res0[0] > 0 ? info.res[0] / info.res0[0] : 1.0;
+        for (int q = 0; q < 4; q++) r->coef[q] = info.coef[q];
         int fin = info.status ? CSU_SRV_FAILED
                   : info.done == 1 ? CSU_SRV_CONVERGED
                   : (info.done == 2 || info.iter >= r->max_iters) ? CSU_SRV_MAXITER : 0;
@@ -271,6 +274,7 @@ static int retire(csu_srv* s, Group* g)
         if ((st = csu_pack_get_state(g->pack, (int)k, r->U.data()))) return st;
         r->state = fin;
         r->t_end = s->now();
+        s->finished.push_back(r->id);
         if (fin == CSU_SRV_FAILED) {
             char msg[96];
             snprintf(msg, sizeof(msg), "the state became non-finite by iteration %d", info.iter);
@@ -367,6 +371,7 @@ extern "C" int csu_srv_step(csu_srv* s, int* n_running, int* n_queued)
         if (rd == 2) { // its layout failed or it exceeds the budget (status and message set by prepare)
             r->state = CSU_SRV_FAILED;
             r->t_start = r->t_end = s->now();
+            s->finished.push_back(r->id);
             it = s->queue.erase(it);
             continue;
         }
@@ -432,6 +437,7 @@ extern "C" int csu_srv_info(csu_srv* s, long long id, csu_srv_request_info* out)
     out->t_end = r->t_end;
     out->n_cells = r->nc;
     out->status = r->status;
+    for (int q = 0; q < 4; q++) out->coef[q] = r->coef[q];
     return CSU_OK;
 }
 
@@ -444,6 +450,18 @@ extern "C" int csu_srv_message(csu_srv* s, long long id, char* buf, int cap)
         return CSU_ERR_INPUT;
     }
     snprintf(buf, (size_t)cap, "%s", it->second->message);
+    return CSU_OK;
+}
+
+extern "C" int csu_srv_poll(csu_srv* s, long long* ids, int cap, int* n)
+{
+    if (!s || !n || cap < 0 || (cap > 0 && !ids)) return CSU_ERR_INPUT;
+    int k = 0;
+    while (k < cap && !s->finished.empty()) {
+        ids[k++] = s->finished.front();
+        s->finished.pop_front();
+    }
+    *n = k;
     return CSU_OK;
 }
 
@@ -487,6 +505,7 @@ extern "C" int csu_srv_cancel(csu_srv* s, long long id)
     // a queued request leaves the queue at the next step (a preparation thread may still hold it)
     r->state = CSU_SRV_CANCELLED;
     r->t_end = s->now();
+    s->finished.push_back(r->id);
     if (r->t_start == 0) r->t_start = r->t_end;
     fail_req(r, CSU_ERR_CANCELLED, "cancelled by the caller");
     return CSU_OK;

@@ -274,6 +274,8 @@ int csu_stats(csu_ctx* ctx, long long* kernel_launches, long long* device_bytes)
  * solve are block aligned and every reduction (norms, time step, coefficients, DPLUR early exit,
  * convergence stop) is per solve, so a solve's iterations are bit-identical alone and in a pack.
  * csu_iterate advances every solve of a pack; a converged or failed solve is frozen while the others run.
+ * On a pack, csu_iterate returns once the iterations are queued on the device (its n_done reports the
+ * iterations queued); csu_pack_info / csu_pack_infos / csu_pack_get_state wait for them.
  */
 typedef struct csu_prep csu_prep;
 typedef struct csu_solve_info {
@@ -344,6 +346,7 @@ typedef struct csu_srv_request_info {
     double t_submit, t_start, t_end;
     int status;              /* CSU_OK, or why it failed or stopped: CSU_ERR_OOM (over the budget),
                                 CSU_ERR_INPUT (its layout failed), CSU_ERR_NONFINITE, CSU_ERR_CANCELLED */
+    double coef[4];          /* Cx_p, Cx_v, Cy_p, Cy_v of its last iteration (solverCalcCoeff3)           */
 } csu_srv_request_info;
 
 int csu_srv_create(const csu_srv_config* cfg, csu_srv** out);
@@ -359,6 +362,9 @@ int csu_srv_take(csu_srv* s, long long id, double* U);      /* final state (refe
 int csu_srv_cancel(csu_srv* s, long long id);
 /* The message of a failed or cancelled request (also for failures met on a preparation thread). */
 int csu_srv_message(csu_srv* s, long long id, char* buf, int cap);
+/* Requests that reached a final state (converged, failed, iteration cap, cancelled) since the last call, in
+ * the order they got there: up to cap ids into ids, their number into *n (the rest wait for the next call). */
+int csu_srv_poll(csu_srv* s, long long* ids, int cap, int* n);
 int csu_srv_totals(csu_srv* s, long long* solve_iterations, long long* cell_updates, long long* used_bytes);
 /* host seconds spent rebuilding packs, iterating and polling, and the number of rebuilds */
 int csu_srv_times(csu_srv* s, double* rebuild_s, double* iterate_s, double* poll_s, int* rebuilds);
