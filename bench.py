@@ -9,6 +9,11 @@ of one cell).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl csu|reference]
 
+The default line also carries `serve`: the serving headline (converged solves/hr of the continuous-batching
+server with FP32 DPLUR blocks against the plain FP64 path one solve at a time, p50/p99 time-to-converge,
+converged-state and force-coefficient differences) on a bounded seeded stream (csu_b200.servebench);
+`--serve` runs a larger stream alone.
+
 N > 1 (one process per GPU under torch.distributed.run) runs independent replicas of the solve, one per
 GPU: the path has no exchange step at this size, so there is no collective in the timed region (weak
 scaling). `--impl reference` times the reference solver compiled from its own C sources
@@ -196,6 +201,24 @@ def reference_arm(args, rank):
     return 0
 
 
+SERVE_DEFAULT = {"n": 24, "cells_hi": 6e4, "rate": 20.0}
+
+
+def serve_summary(n, cells_hi, rate):
+    """The serving comparison of csu_b200.servebench on a bounded stream, summarized for the bench line."""
+    from csu_b200 import servebench
+    t0 = time.perf_counter()
+    out = servebench.run(n=n, cells_hi=cells_hi, rate=rate)
+    b, p = out["batched"], out["plain"]
+    keys = ("solves_per_hour", "converged", "requests", "failed", "p50_s", "p99_s", "makespan_s",
+            "cell_updates_per_s")
+    return {"metric": "converged solves/hr", "unit": "solves/hr",
+            "vs_plain_fp64": b["solves_per_hour"] / p["solves_per_hour"] if p["solves_per_hour"] else None,
+            "batched_mixed": {k: b[k] for k in keys}, "plain_fp64": {k: p[k] for k in keys},
+            "state_diff_rel": out["state_diff_rel"], "force_coef_diff_rel": out["coef_diff_rel"],
+            "workload": out["workload"], "wall_s": time.perf_counter() - t0}
+
+
 def serve_arm(args):
     """Serving stream (csu_b200.servebench): requests of four geometry families arriving as a Poisson stream,
     served by the continuous-batching server (packs, FP32 DPLUR blocks) and by the plain FP64 path one solve
@@ -228,6 +251,8 @@ def main():
     ap.add_argument("--requests", type=int, default=40)
     ap.add_argument("--cells-hi", type=float, default=2e5)
     ap.add_argument("--rate", type=float, default=5.0, help="serving stream: Poisson arrivals per second")
+    ap.add_argument("--no-serve", action="store_true",
+                    help="leave the bounded serving comparison out of the default line")
     args = ap.parse_args()
     if args.serve:
         return serve_arm(args)
@@ -271,6 +296,7 @@ def main():
         torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
     launches = eng.stats()["kernel_launches"] - launches0
+    ws_mb = eng.stats()["device_bytes"] / 1e6
     ms = max_over_ranks(ms, dist, "cuda")
     if dist:
         dist.barrier()
@@ -321,21 +347,30 @@ def main():
             cpu = {"value": nc_r * n_it / dt_r, "unit": METRIC, "cores": threads, "kind": "reference",
                    "sample": "%d DPLUR iterations of the full 160k-cell ramp (%.1f s)" % (n_it, dt_r)}
 
+    # the serving headline (converged solves/hr, batched mixed precision vs plain FP64 one solve at a time)
+    # on a bounded stream, after the timed region
+    serve = None
+    if rank == 0 and world == 1 and not args.no_serve:
+        eng.close()
+        eng = None
+        serve = serve_summary(**SERVE_DEFAULT)
+
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": workload_config(nc, case.n_faces, world),
-                "working_set_mb": eng.stats()["device_bytes"] / 1e6,
+                "working_set_mb": ws_mb,
                 "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
                              "alg_bytes_per_launch": ab[dom], "ms_per_launch": per[dom]},
                 "kernel_ms_per_launch": per,
                 "kernel_ms_share": {n: share[n] / max(sum(share.values()), 1e-30) for n in names},
                 "e2e": {"value": e2e, "unit": METRIC, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-                "gpu_launches": launches, "clocks": clk.summary(), "cpu_baseline": cpu}
+                "gpu_launches": launches, "clocks": clk.summary(), "cpu_baseline": cpu, "serve": serve}
         print(json.dumps(line))
-    eng.close()
+    if eng is not None:
+        eng.close()
     if dist:
         dist.destroy_process_group()
     return 0

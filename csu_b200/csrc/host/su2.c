@@ -442,35 +442,161 @@ fail:
 
 /* saCalcD (sa.c:703-793): brute-force distance from the cell centroid to every wall edge (flags 3, 4).
  * Kept O(Ncell * Nwall) so the minimum is taken over the same candidates in the same order. */
+/* saCalcD (sa.c:703-793): each cell's distance d = min over the wall faces (flags 3, 4) of the reference's
+ * point-to-segment expression from the cell's vertex-average centre, starting from 1e6. A minimum does not
+ * depend on the order of its terms, so any search that evaluates that same expression on a set of faces
+ * containing the nearest ones gives the reference's d bit for bit. The faces go into a uniform grid of
+ * buckets over their bounding box (each face into every bucket its own bounding box touches); a cell looks
+ * at the buckets ring by ring around the bucket nearest to it and stops once no face beyond the current ring
+ * can be closer: every bucket of ring k (k >= 1) lies at least (k - 1) bucket widths from the cell, which
+ * must exceed the best distance found, with a relative margin far above rounding. Cost: about the number of
+ * faces in a few buckets per cell instead of all of them (O(N_cells * N_wall) in the reference). */
+typedef struct {
+    double p0x, p0y, p1x, p1y;
+} wall_seg;
+
+static double seg_distance(const wall_seg* w, double xv, double yv)
+{
+    double num = (w->p1x - w->p0x) * (xv - w->p0x) + (w->p1y - w->p0y) * (yv - w->p0y);
+    double den = (w->p1x - w->p0x) * (w->p1x - w->p0x) + (w->p1y - w->p0y) * (w->p1y - w->p0y);
+    double t = num / den;
+    if (t > 1.) t = 1.;
+    else if (t < 0.) t = 0.;
+    double dx = (w->p1x - w->p0x) * t + w->p0x - xv;
+    double dy = (w->p1y - w->p0y) * t + w->p0y - yv;
+    return sqrt(dx * dx + dy * dy);
+}
+
 void csu_mesh_wall_distance(csu_mesh* m)
 {
     if (!m->wall_dist) m->wall_dist = malloc(sizeof(double) * m->n_cells);
     for (int i = 0; i < m->n_cells; i++) m->wall_dist[i] = 1e6;
-    int base = 0;
+    int nw = 0, base = 0;
+    for (int k = 0; k < m->n_markers; k++)
+        if (m->marker_flag[k] == CSU_BC_WALL || m->marker_flag[k] == CSU_BC_WALLT) nw += m->marker_nbf[k];
+    if (nw == 0) return;
+    wall_seg* w = malloc(sizeof(wall_seg) * nw);
+    double xlo = 1e300, xhi = -1e300, ylo = 1e300, yhi = -1e300;
+    nw = 0;
     for (int k = 0; k < m->n_markers; k++) {
         int nb = m->marker_nbf[k];
         if (m->marker_flag[k] == CSU_BC_WALL || m->marker_flag[k] == CSU_BC_WALLT) {
-            for (int i = 0; i < m->n_cells; i++) {
-                double xv, yv;
-                csu_mesh_center(m, i, &xv, &yv);
-                double dmin = m->wall_dist[i];
-                for (int j = 0; j < nb; j++) {
-                    const int* bf = m->bface + 3 * (base + j);
-                    double p0x = m->xy[2 * bf[0]], p0y = m->xy[2 * bf[0] + 1];
-                    double p1x = m->xy[2 * bf[1]], p1y = m->xy[2 * bf[1] + 1];
-                    double num = (p1x - p0x) * (xv - p0x) + (p1y - p0y) * (yv - p0y);
-                    double den = (p1x - p0x) * (p1x - p0x) + (p1y - p0y) * (p1y - p0y);
-                    double t = num / den;
-                    if (t > 1.) t = 1.;
-                    else if (t < 0.) t = 0.;
-                    double dx = (p1x - p0x) * t + p0x - xv;
-                    double dy = (p1y - p0y) * t + p0y - yv;
-                    double d = sqrt(dx * dx + dy * dy);
-                    if (dmin > d) dmin = d;
-                }
-                m->wall_dist[i] = dmin;
+            for (int j = 0; j < nb; j++) {
+                const int* bf = m->bface + 3 * (base + j);
+                wall_seg* g = &w[nw++];
+                g->p0x = m->xy[2 * bf[0]];
+                g->p0y = m->xy[2 * bf[0] + 1];
+                g->p1x = m->xy[2 * bf[1]];
+                g->p1y = m->xy[2 * bf[1] + 1];
+                xlo = fmin(xlo, fmin(g->p0x, g->p1x));
+                xhi = fmax(xhi, fmax(g->p0x, g->p1x));
+                ylo = fmin(ylo, fmin(g->p0y, g->p1y));
+                yhi = fmax(yhi, fmax(g->p0y, g->p1y));
             }
         }
         base += nb;
     }
+    /* about two faces per bucket, buckets as square as the box allows */
+    double wx = xhi - xlo, wy = yhi - ylo;
+    double span = fmax(fmax(wx, wy), 1e-300);
+    double h = fmax(sqrt(wx * wy / (0.5 * nw)), span / (2.0 * nw));
+    if (!(h > 0) || !isfinite(h)) h = span;
+    int gx = (int)fmin(fmax(ceil(wx / h), 1.0), 4096.0), gy = (int)fmin(fmax(ceil(wy / h), 1.0), 4096.0);
+    double hx = fmax(wx / gx, 1e-300), hy = fmax(wy / gy, 1e-300);
+    /* bucket lists: counts, prefix sums, fill */
+    int nbk = gx * gy;
+    int* cnt = calloc(nbk + 1, sizeof(int));
+    for (int pass = 0; pass < 2; pass++) {
+        int* fillp = NULL;
+        int* items = NULL;
+        if (pass == 1) {
+            for (int b = 0; b < nbk; b++) cnt[b + 1] += cnt[b];
+            fillp = malloc(sizeof(int) * nbk);
+            memcpy(fillp, cnt, sizeof(int) * nbk);
+            items = malloc(sizeof(int) * (cnt[nbk] > 0 ? cnt[nbk] : 1));
+        }
+        for (int s2 = 0; s2 < nw; s2++) {
+            const wall_seg* g = &w[s2];
+            int i0 = (int)floor((fmin(g->p0x, g->p1x) - xlo) / hx), i1 = (int)floor((fmax(g->p0x, g->p1x) - xlo) / hx);
+            int j0 = (int)floor((fmin(g->p0y, g->p1y) - ylo) / hy), j1 = (int)floor((fmax(g->p0y, g->p1y) - ylo) / hy);
+            i0 = i0 < 0 ? 0 : (i0 >= gx ? gx - 1 : i0);
+            i1 = i1 < 0 ? 0 : (i1 >= gx ? gx - 1 : i1);
+            j0 = j0 < 0 ? 0 : (j0 >= gy ? gy - 1 : j0);
+            j1 = j1 < 0 ? 0 : (j1 >= gy ? gy - 1 : j1);
+            for (int j = j0; j <= j1; j++)
+                for (int i = i0; i <= i1; i++) {
+                    if (pass == 0) cnt[j * gx + i + 1]++;
+                    else items[fillp[j * gx + i]++] = s2;
+                }
+        }
+        if (pass == 1) {
+            free(fillp);
+            /* search */
+            int last = -1; /* the previous cell's nearest face: a first candidate for the next cell */
+            for (int c = 0; c < m->n_cells; c++) {
+                double xv, yv;
+                csu_mesh_center(m, c, &xv, &yv);
+                int ic = (int)floor((xv - xlo) / hx), jc = (int)floor((yv - ylo) / hy);
+                ic = ic < 0 ? 0 : (ic >= gx ? gx - 1 : ic);
+                jc = jc < 0 ? 0 : (jc >= gy ? gy - 1 : jc);
+                /* the point's distance to the grid's x and y ranges (0 inside) */
+                const double dxg = xv < xlo ? xlo - xv : (xv > xhi ? xv - xhi : 0.0);
+                const double dyg = yv < ylo ? ylo - yv : (yv > yhi ? yv - yhi : 0.0);
+                double best = m->wall_dist[c];
+                int arg = -1;
+                if (last >= 0) {
+                    double d = seg_distance(&w[last], xv, yv);
+                    if (best > d) {
+                        best = d;
+                        arg = last;
+                    }
+                }
+                const int kmax = gx > gy ? gx : gy;
+                for (int k = 0; k <= kmax; k++) {
+                    const double lim = best * (1.0 + 1e-9) + 1e-300;
+                    if (k >= 1) {
+                        /* every bucket of ring k or beyond is k - 1 columns beyond the point's column (x
+                         * distance >= (k-1) hx + dxg, y distance >= dyg) or k - 1 rows beyond its row */
+                        double lb = 1e300;
+                        if (ic - k >= 0 || ic + k < gx) {
+                            double a = (k - 1) * hx + dxg;
+                            lb = fmin(lb, sqrt(a * a + dyg * dyg));
+                        }
+                        if (jc - k >= 0 || jc + k < gy) {
+                            double b = (k - 1) * hy + dyg;
+                            lb = fmin(lb, sqrt(dxg * dxg + b * b));
+                        }
+                        if (lb > lim) break;
+                    }
+                    for (int j = jc - k; j <= jc + k; j++) {
+                        if (j < 0 || j >= gy) continue;
+                        const double by0 = ylo + j * hy;
+                        const double ddy = yv < by0 ? by0 - yv : (yv > by0 + hy ? yv - by0 - hy : 0.0);
+                        if (ddy > lim) continue;
+                        int step = (j == jc - k || j == jc + k) ? 1 : 2 * k;
+                        for (int i = ic - k; i <= ic + k; i += (step > 0 ? step : 1)) {
+                            if (i < 0 || i >= gx) continue;
+                            const int b = j * gx + i;
+                            if (cnt[b] == cnt[b + 1]) continue;
+                            const double bx0 = xlo + i * hx;
+                            const double ddx = xv < bx0 ? bx0 - xv : (xv > bx0 + hx ? xv - bx0 - hx : 0.0);
+                            if (ddx * ddx + ddy * ddy > lim * lim) continue;
+                            for (int q = cnt[b]; q < cnt[b + 1]; q++) {
+                                double d = seg_distance(&w[items[q]], xv, yv);
+                                if (best > d) {
+                                    best = d;
+                                    arg = items[q];
+                                }
+                            }
+                        }
+                    }
+                }
+                if (arg >= 0) last = arg;
+                m->wall_dist[c] = best;
+            }
+            free(items);
+        }
+    }
+    free(cnt);
+    free(w);
 }

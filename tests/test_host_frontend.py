@@ -70,6 +70,23 @@ def test_bench_mesh_integer_exact(native):
     assert np.array_equal(case.initial_state(), ref.get_U())
 
 
+@pytest.mark.parametrize("gen", ["plate", "airfoil", "cylinder", "bump"])
+def test_wall_distance_bit_exact(native, gen):
+    """The bucketed wall-distance search gives saCalcD's distances (sa.c:703-793) bit for bit on generated
+    SA meshes with curved, clustered and stretched walls."""
+    import csu_b200
+    from csu_b200 import meshgen
+    kw = {"viscous": "sa", "re": 2e6}
+    su2, inp = {"plate": lambda: meshgen.plate(ni=120, nj=70, y1=1e-5),
+                "airfoil": lambda: meshgen.airfoil(ncells=12000, y1=1e-5, **kw),
+                "cylinder": lambda: meshgen.cylinder(ncells=9000, tri_fraction=0.3, **kw),
+                "bump": lambda: meshgen.bump(ncells=9000, **kw)}[gen]()
+    wd = casekit.write_case(inp, su2, "wd" + gen)
+    case = csu_b200.Case.load(wd)
+    m = _ref(wd).mesh()
+    assert case.wall_dist is not None and np.array_equal(case.wall_dist, m["wall_dist"])
+
+
 def _ref_input(path):
     """The reference's own keyword parser, inputInit (input.c:7-95), through the built reference."""
     from oracle.refharness import LIB, available
