@@ -300,7 +300,7 @@ static void plan(csu_ctx* x, Arena& a)
     x->d_prm = carve<Prm>(a, x->nsolve);
     s.dbg_ghost = carve<double>(a, (size_t)(nb > 0 ? nb : 1) * (nv + 1));
     s.lsq_x87 = carve<unsigned long long>(a, 1);
-    s.dQ = x->cfg.sst && x->cfg.time_scheme == CSU_TS_LUSGS ? carve<double>(a, (size_t)6 * nc) : nullptr;
+    s.dQ = x->cfg.sst && x->cfg.time_scheme != CSU_TS_RK ? carve<double>(a, (size_t)6 * nc) : nullptr;
     s.gfix = carve<int2>(a, (size_t)nc * (nv + 1)); // at most one entry per cell and variable (and T)
     s.gfix_n = carve<unsigned>(a, 2);
     if (!x->is_pack) {
@@ -545,9 +545,8 @@ static int validate_config(const char* who, const csu_config* cfg, int* model_ou
         csu_set_error("%s: nvar %d does not match the turbulence model", who, cfg->nvar);
         return CSU_ERR_INPUT;
     }
-    if (model == 2 && (cfg->flux == CSU_FLUX_ROE || cfg->time_scheme == CSU_TS_DPLUR)) {
-        csu_set_error("%s: SST supports RK and LU-SGS time stepping with the AUSM family (the reference has no "
-                      "Roe branch for SST and calls 4x4 DPLUR blocks with 6 variables)", who);
+    if (model == 2 && cfg->flux == CSU_FLUX_ROE) {
+        csu_set_error("%s: SST with the AUSM family only (the reference has no Roe branch for SST)", who);
         return CSU_ERR_UNSUPPORTED;
     }
     if (cfg->time_scheme == CSU_TS_RK && !(cfg->stages >= 1 && cfg->stages <= 5)) {
@@ -1044,9 +1043,9 @@ static void launch_iteration(csu_ctx* x)
         tmark(x, KPRIM);
         launch_finalize<MODEL>(x, 1);
     } else {
-        // the SA blocks and diagonal need the face eddy viscosity of k_flux; the others only the iteration's
-        // start state
-        constexpr bool early = MODEL != 1;
+        // the SA and SST blocks and diagonal need the face eddy viscosity of k_flux (SST's diagonal also the
+        // gradients, for its source Jacobians); the Euler/laminar ones only the iteration's start state
+        constexpr bool early = MODEL == 0;
         const bool grad = c.order == 2 || x->prm.visc;
         if (!x->timing) cudaEventRecord(x->ev_fork, x->stream);
         if (grad) launch_grad<MODEL>(x, false);
@@ -1674,7 +1673,7 @@ extern "C" int csu_dump(csu_ctx* x, int what, double* out)
     }
     case CSU_DUMP_SST_JAC: {
         if (!x->st.dQ) {
-            csu_set_error("csu_dump: no SST source Jacobians in this context (SST with LU-SGS only)");
+            csu_set_error("csu_dump: no SST source Jacobians in this context (SST with LU-SGS or DPLUR only)");
             return CSU_ERR_STATE;
         }
         CK(d2h(a, x->st.dQ, (size_t)6 * nc));

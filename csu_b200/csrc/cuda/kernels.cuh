@@ -948,8 +948,11 @@ __global__ void __launch_bounds__(BLOCK) k_impl(const Prm* __restrict__ P, const
         if (WITH_R) {
             gather_residual<MODEL>(p, m, s, c, P, R);
             storeR<MODEL>(s, nc, c, R);
+        }
+        {
             if constexpr (MODEL == 2) {
-                // the SST source Jacobians of the LU-SGS diagonal (sstInterSource, sst.c:643-680)
+                // the SST source Jacobians of the implicit diagonal (sstInterSource, sst.c:643-680): LU-SGS
+                // as the reference, DPLUR as the extension's k-omega diagonal block
                 if (s.dQ) {
                     double4 gx = s.G4x[c], gy = s.G4y[c];
                     double sgx[4] = {gx.y, gx.z, s.Gxx[c], s.Gxx[(size_t)nc + c]};
@@ -1061,6 +1064,10 @@ __global__ void __launch_bounds__(BLOCK, 3) k_blocks(const Prm* __restrict__ P, 
     double E = Un[3] / rho;
     aux_flux<NV>(Un, Pn[3], nx, ny, F0);
     double ee0 = E - 0.5 * (uu * uu + vv * vv);
+    // SST (an extension: the reference's SST DPLUR multiplies 4x4 blocks into six variables, implicit.c:
+    // 990-1000 with 938-972): the energy holds the turbulent kinetic energy, as in its SST delta flux
+    // (implicitCalcDeltaFlux_sst, implicit.c:1048-1118)
+    if constexpr (MODEL == 2) ee0 = ee0 - Un[4] / rho;
     double A[NV * NV];
 #pragma unroll
     for (int mm = 0; mm < NV; mm++) {
@@ -1071,6 +1078,7 @@ __global__ void __launch_bounds__(BLOCK, 3) k_blocks(const Prm* __restrict__ P, 
         double v2 = Uq[2] / r2;
         double E2 = Uq[3] / r2;
         double ee1 = E2 - 0.5 * (u2 * u2 + v2 * v2);
+        if constexpr (MODEL == 2) ee1 = ee1 - Uq[4] / r2;
         double T = e2Taprox(p.gas, ee0, Pn[4], ee1);
         double pr = p.gas.R * r2 * T;
         aux_flux<NV>(Uq, pr, nx, ny, F);
@@ -1079,8 +1087,9 @@ __global__ void __launch_bounds__(BLOCK, 3) k_blocks(const Prm* __restrict__ P, 
     }
     double cc = T2c(p.gas, Pn[4]);
     double ra = p.w_imp * (fabs(nx * Pn[1] + ny * Pn[2]) + cc) * dS;
-    if constexpr (MODEL == 1) {
-        // implicitUpdateA_sa (implicit.c:920-928): always viscous, with the face eddy viscosity
+    if constexpr (MODEL >= 1) {
+        // implicitUpdateA_sa (implicit.c:920-928): always viscous, with the face eddy viscosity (SST: the
+        // same radius with its own eddy viscosity)
         double Pc[NP];
         loadP<MODEL>(s, nc, c, Pc);
         double r = (Pc[0] + Pn[0]) * 0.5;
@@ -1162,9 +1171,10 @@ __global__ void __launch_bounds__(SB) k_sweep(const Prm* __restrict__ P, const _
             double cfl = cfl_at(p, sc->iter);
             double dt = p.implicit_local_dt ? s.dtl[c] * cfl : bitsd(sc->dtmin_bits) * cfl;
             double D = s.dpart[c] + m.omega[c] / dt;
+            // y = D x + sum_j A_j x_j; SST keeps the off-diagonal sum alone (its diagonal is a block)
             double y[NV];
 #pragma unroll
-            for (int k = 0; k < NV; k++) y[k] = D * xo[k];
+            for (int k = 0; k < NV; k++) y[k] = MODEL == 2 ? 0.0 : D * xo[k];
             // Slots 0-2 are gathered unconditionally (a slot without a face reads the cell itself and a zero
             // block, both in bounds, and is not summed), so their index and neighbour loads issue together
             // instead of one dependent chain per face; slot 3 only exists in quadrilaterals.
@@ -1203,8 +1213,32 @@ __global__ void __launch_bounds__(SB) k_sweep(const Prm* __restrict__ P, const _
                 }
             }
             const double w = 2. / 3.;
+            if constexpr (MODEL == 2) {
+                // SST (extension): the diagonal block is D on the mean flow and, on k and omega, D minus the
+                // source Jacobians (the 2x2 block of the LU-SGS diagonal, implicit.c:323-345, with its
+                // coupling to rho): x* = Dblock^-1 (-R - sum_j A_j x_j), then x += w (x* - x)
+                double z[NV], xs[NV];
 #pragma unroll
-            for (int k = 0; k < NV; k++) xn[k] = w * (-R[k] - y[k]) / D + xo[k];
+                for (int k = 0; k < NV; k++) z[k] = -R[k] - y[k];
+#pragma unroll
+                for (int k = 0; k < 4; k++) xs[k] = z[k] / D;
+                const double a = D - s.dQ[(size_t)nc + c], b = -s.dQ[(size_t)2 * nc + c];
+                const double cq = -s.dQ[(size_t)4 * nc + c], dq = D - s.dQ[(size_t)5 * nc + c];
+                const double Ak = z[4] + s.dQ[c] * xs[0], Bw = z[5] + s.dQ[(size_t)3 * nc + c] * xs[0];
+                const double det = a * dq - b * cq;
+                if (fabs(det) < 1e-14) {
+                    xs[4] = z[4] / D;
+                    xs[5] = z[5] / D;
+                } else {
+                    xs[4] = (Ak * dq - Bw * b) / det;
+                    xs[5] = (-Ak * cq + Bw * a) / det;
+                }
+#pragma unroll
+                for (int k = 0; k < NV; k++) xn[k] = xo[k] + w * (xs[k] - xo[k]);
+            } else {
+#pragma unroll
+                for (int k = 0; k < NV; k++) xn[k] = w * (-R[k] - y[k]) / D + xo[k];
+            }
             dmax = fabs(xn[0] - xo[0]);
         }
         xn4[c] = make_double4(xn[0], xn[1], xn[2], xn[3]);

@@ -198,7 +198,8 @@ int csu_tube_run(csu_ctx* ctx, double tmax, int* steps, double* t_final);
  *                                               least squares could not decide and left to the integer x87
  *                                               model (no reference counterpart: a diagnostic of this engine)
  *  CSU_DUMP_SST_JAC 6*ncells                    SST source Jacobians dQkdr, dQkdrk, dQkdro, dQodr, dQodrk,
- *                                               dQodro [6][cell] of the last LU-SGS iteration (sst.c:643-680)
+ *                                               dQodro [6][cell] of the last LU-SGS or DPLUR iteration
+ *                                               (sst.c:643-680)
  *  CSU_DUMP_BVISC   nbfaces*4 [bface][k]        viscous flux of each boundary face: x and y momentum, energy,
  *                                               transported scalar (components 1..4 of boundaryFaceViscFlux,
  *                                               laminar.c:128-346; saBoundaryFaceViscFlux, sa.c:370-692;

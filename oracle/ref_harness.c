@@ -197,6 +197,12 @@ void ref_sst_jac(double* J)
     for (int q = 0; q < 6; q++) memcpy(J + (size_t)q * n, a[q], sizeof(double) * n);
 }
 
+/* the face eddy viscosity of the last solverCalcR (SA, SST): miT[face], mesh->con order */
+void ref_get_miT(double* miT)
+{
+    memcpy(miT, g->miT, sizeof(double) * g->mesh->Ncon);
+}
+
 void ref_get_R(double* R)
 {
     for (int k = 0; k < g->Nvar; k++)

@@ -108,6 +108,12 @@ class Ref:
         self.L.ref_sst_jac(_p(J))
         return J.reshape(6, self.nc)
 
+    def miT(self):
+        """Face eddy viscosity of the last calc_R (SA, SST), per face in mesh->con order."""
+        a = np.zeros(self.nf)
+        self.L.ref_get_miT(_p(a))
+        return a
+
     def implicit_D(self):
         D, dtl = np.zeros(self.nc), np.zeros(self.nc)
         self.L.ref_implicit_D(_p(D), _p(dtl))

@@ -1,0 +1,161 @@
+"""SST under DPLUR, an extension: the reference's implicitCalcDPLUR calls the 4x4 implicitUpdateA for SST
+(implicit.c:990-1000) while implicitMultA reads six variables (938-972), so it has no defined result to
+match. The extension's operator, restated here in numpy as its checker:
+
+  blocks    A_j = 1/2 dF_n/dU (U_j) dS - 1/2 ra I, forward differences (h = 1e-6) of the six-variable
+            convective flux (implicitAuxCalcFlux2_sst, implicit.c:183-191 form) with the energy holding k,
+            as the reference's SST delta flux does (implicit.c:1048-1118); ra = wImp (|V_n| + c) dS plus the
+            viscous radius with the face eddy viscosity (implicitUpdateA_sa's form, implicit.c:920-928)
+  diagonal  D (implicitCalcD, implicit.c:19-181) on the mean flow; on k and omega the 2x2 block D - dQ of
+            the SST source Jacobians with their rho coupling (the LU-SGS diagonal, implicit.c:323-345)
+  sweeps    x* = Dblock^-1 (-R - sum_j A_j x_j), x += 2/3 (x* - x), stop once max |dx_0| < 1e-14
+
+The reference supplies R, the primitives, D, the source Jacobians and the face eddy viscosity of the same
+state (through its harness); the engine's first increment must agree with the restatement. Then a run of
+the extension with FP32 blocks is checked to move the residual down without leaving finite values."""
+import numpy as np
+import pytest
+
+import casekit
+
+pytestmark = pytest.mark.gpu
+
+KV = {"restart": "0", "sa": "0", "sst": "1", "CFL": "2.0"}
+
+
+def _restated_increment(ref, m, U, P, R, D, dQ, miT, gamma, Rg, w_imp, pr, pr_t, n_lin):
+    nc, nv = U.shape[1], 6
+    cp = gamma * Rg / (gamma - 1)
+    cv = cp - Rg
+    xy = m["xy"].reshape(-1, 2)
+    nodes = m["nodes"].reshape(-1, 4)
+    npts = m["npts"]
+    cen = np.zeros((nc, 2))
+    for c in range(nc):
+        cen[c] = xy[nodes[c, :npts[c]]].sum(axis=0) / npts[c]
+    con = m["con"].reshape(-1, 4)
+    f = m["f"].reshape(-1, 4)
+    nint = m["nint"]
+    h = 1.0e-6
+
+    def aux(Uq, p, nx, ny):
+        V = (nx * Uq[1] + ny * Uq[2]) / Uq[0]
+        return np.array([Uq[0] * V, Uq[1] * V + nx * p, Uq[2] * V + ny * p, (Uq[3] + p) * V, Uq[4] * V,
+                         Uq[5] * V])
+
+    def sutherland(T):
+        return 1.458e-6 * T * np.sqrt(T) / (T + 110.4)
+
+    blocks = []  # per cell: list of (neighbour, 6x6)
+    for c in range(nc):
+        row = []
+        for j in range(nint[c]):
+            sf = f[c, j]
+            face = abs(sf) - 1
+            if sf > 0:
+                e0, e1, p0, p1 = con[face]
+            else:
+                e1, e0, p1, p0 = con[face]
+            dSx, dSy = xy[p1, 1] - xy[p0, 1], -(xy[p1, 0] - xy[p0, 0])
+            dS = np.sqrt(dSx * dSx + dSy * dSy)
+            nx, ny = dSx / dS, dSy / dS
+            Un, Pn = U[:, e1], P[e1]
+            rho = Un[0]
+            uu, vv, E = Un[1] / rho, Un[2] / rho, Un[3] / rho
+            F0 = aux(Un, Pn[3], nx, ny)
+            ee0 = E - 0.5 * (uu * uu + vv * vv)
+            ee0 = ee0 - Un[4] / rho
+            A = np.zeros((nv, nv))
+            for mm in range(nv):
+                Uq = Un.copy()
+                Uq[mm] = Un[mm] + h
+                r2 = Uq[0]
+                u2, v2, E2 = Uq[1] / r2, Uq[2] / r2, Uq[3] / r2
+                ee1 = E2 - 0.5 * (u2 * u2 + v2 * v2)
+                ee1 = ee1 - Uq[4] / r2
+                T = Pn[4] + (ee1 - ee0) / cv
+                F = aux(Uq, Rg * r2 * T, nx, ny)
+                A[:, mm] = 0.5 * (F - F0) * dS / h
+            cc = np.sqrt(gamma * Rg * Pn[4])
+            ra = w_imp * (abs(nx * Pn[1] + ny * Pn[2]) + cc) * dS
+            r = (P[e0, 0] + Pn[0]) * 0.5
+            Tf = (P[e0, 4] + Pn[4]) * 0.5
+            L = np.sqrt(((cen[e1] - cen[e0]) ** 2).sum())
+            ra += max(4 / (3 * r), gamma / r) * (sutherland(Tf) / pr + miT[face] / pr_t) * dS / L
+            A -= 0.5 * ra * np.eye(nv)
+            row.append((e1, A))
+        blocks.append(row)
+    x = np.zeros((nv, nc))
+    w = 2.0 / 3.0
+    for sweep in range(n_lin):
+        xn = np.empty_like(x)
+        for c in range(nc):
+            z = -R[:, c].copy()
+            for nb, A in blocks[c]:
+                z -= A @ x[:, nb]
+            xs = np.empty(nv)
+            xs[:4] = z[:4] / D[c]
+            a, b = D[c] - dQ[1, c], -dQ[2, c]
+            cq, dq = -dQ[4, c], D[c] - dQ[5, c]
+            Ak, Bw = z[4] + dQ[0, c] * xs[0], z[5] + dQ[3, c] * xs[0]
+            det = a * dq - b * cq
+            if abs(det) < 1e-14:
+                xs[4], xs[5] = z[4] / D[c], z[5] / D[c]
+            else:
+                xs[4], xs[5] = (Ak * dq - Bw * b) / det, (-Ak * cq + Bw * a) / det
+            xn[:, c] = x[:, c] + w * (xs - x[:, c])
+        dmax = np.max(np.abs(xn[0] - x[0]))
+        x = xn
+        if dmax < 1e-14:
+            break
+    return x
+
+
+def test_sst_dplur_first_increment(native):
+    import csu_b200
+    from oracle.refharness import Ref, available
+    if not available():
+        pytest.skip("reference build oracle/_ref missing")
+    # a non-uniform SST state: three RK iterations of the engine from the free stream
+    wd_rk = casekit.materialize("caseBL_turb", KV)
+    case_rk = csu_b200.Case.load(wd_rk)
+    rk = csu_b200.Engine(case_rk)
+    rk.iterate(3)
+    U = rk.get_state()
+    rk.close()
+    wd = casekit.materialize("caseBL_turb", dict(KV, timeScheme="DPLUR", Nlinear="4"))
+    case = csu_b200.Case.load(wd)
+    eng = csu_b200.Engine(case, state=U)
+    eng.iterate(1)
+    dW = eng.dump("DW")
+    ref = Ref(wd)
+    ref.set_U(U)
+    R = ref.calc_R()
+    P = ref.P()
+    dQ = ref.sst_jac()
+    miT = ref.miT()
+    D, _ = ref.implicit_D()
+    U_clamped = ref.get_U()
+    # the engine's own diagonal and source Jacobians of that state agree with the reference's
+    assert np.max(np.abs(eng.dump("D") - D) / np.abs(D)) < 1e-12
+    assert np.max(np.abs(eng.dump("SST_JAC") - dQ) / (np.abs(dQ).max(axis=1, keepdims=True) + 1e-300)) < 1e-12
+    c = case.config
+    x = _restated_increment(ref, ref.mesh(), U_clamped, P, R, D, dQ, miT, c.gamma, c.gas_r, c.w_imp, c.pr,
+                            c.pr_t, c.n_linear)
+    scale = np.abs(x).max(axis=1, keepdims=True) + 1e-300
+    err = np.max(np.abs(dW - x) / scale)
+    print("SST DPLUR first increment vs restatement: %.3e" % err)
+    assert err < 1e-10
+    eng.close()
+
+
+def test_sst_dplur_fp32_runs(native):
+    """The extension with FP32 blocks and local steps moves the residual down on the SST plate."""
+    import csu_b200
+    wd = casekit.materialize("caseBL_turb", dict(KV, timeScheme="DPLUR", Nlinear="8", CFL="4.0",
+                                                 implicitFP32="1", implicitLocalDt="1"))
+    eng = csu_b200.Engine(csu_b200.Case.load(wd))
+    h = eng.iterate(300)
+    assert np.isfinite(h).all()
+    assert h[-1, 0] < h[0, 0]
+    eng.close()
