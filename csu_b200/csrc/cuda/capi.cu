@@ -127,6 +127,9 @@ struct csu_ctx {
     // Nlinear flips it every iteration); captured on first use, kept until the launch sequence changes
     cudaGraphExec_t graphs[4][2] = {};
     long long graph_launches[4][2] = {};
+    // L2 residency of the DPLUR blocks: the sweeps of an iteration read them again and again, and they fit in
+    // L2 on B200; the window is set on the kernel nodes of the captured iteration graphs
+    cudaAccessPolicyWindow l2win = {};
     Scalars* h_sc = nullptr;   // pinned: solve 0's scalars, read back once at the end of csu_iterate
     int* h_flags = nullptr;    // pinned: halt flags (status, done) of two chunks in flight
     bool snap = false;         // csu_iterate_views: copy the last residual evaluation's primitives/gradients
@@ -592,6 +595,8 @@ static int max_nint(const csu_layout& L)
     return m;
 }
 
+static void plan_l2_window(csu_ctx* x);
+
 static int ctx_setup(csu_ctx* x)
 {
     int st;
@@ -627,6 +632,7 @@ static int ctx_setup(csu_ctx* x)
     if (e != cudaSuccess) return cuda_fail(e, "context setup");
     x->gb_c = (x->L.nc + BLOCK - 1) / BLOCK;
     if (x->L.nint) x->max_ni = max_nint(x->L); // packs set it from their solves
+    plan_l2_window(x);
     if (!x->is_pack && (st = upload_mesh(x))) return st; // packs: pack_build fills the mesh rows
     x->prm = x->prms[0];
     if ((st = upload_prm(x)) || (st = reset_scalars(x, 0))) return st;
@@ -1116,6 +1122,57 @@ static int ensure_hist(csu_ctx* x, int n)
     return write_scalars_n(x, hs.data(), x->nsolve);
 }
 
+// The DPLUR blocks (written once per iteration, read by every sweep) as a persisting L2 window: as much of
+// them as the device lets persist (cudaDevAttrMaxPersistingL2CacheSize), the rest streaming. Only a cache
+// policy: no result depends on it. CSU_L2_PERSIST=0 leaves the L2 alone.
+static void plan_l2_window(csu_ctx* x)
+{
+    x->l2win = cudaAccessPolicyWindow{};
+    const char* env = getenv("CSU_L2_PERSIST");
+    if (env && strcmp(env, "0") == 0) return;
+    void* base = x->st.blocks32 ? (void*)x->st.blocks32 : (void*)x->st.blocks;
+    if (!base || x->cfg.time_scheme != CSU_TS_DPLUR) return;
+    const size_t bytes = (size_t)x->max_ni * x->nv * x->nv * x->L.nc * (x->st.blocks32 ? sizeof(float) : sizeof(double));
+    int max_persist = 0, max_window = 0;
+    if (cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, x->device) != cudaSuccess ||
+        cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, x->device) != cudaSuccess ||
+        max_persist <= 0 || max_window <= 0) {
+        cudaGetLastError();
+        return;
+    }
+    size_t cur = 0;
+    cudaDeviceGetLimit(&cur, cudaLimitPersistingL2CacheSize);
+    const size_t want = std::min(bytes, (size_t)max_persist);
+    if (cur < want && cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    cudaDeviceGetLimit(&cur, cudaLimitPersistingL2CacheSize);
+    const size_t win = std::min(bytes, (size_t)max_window);
+    x->l2win.base_ptr = base;
+    x->l2win.num_bytes = win;
+    x->l2win.hitRatio = (float)std::min(1.0, (double)cur / (double)win);
+    x->l2win.hitProp = cudaAccessPropertyPersisting;
+    x->l2win.missProp = cudaAccessPropertyStreaming;
+}
+
+static void apply_l2_window(csu_ctx* x, cudaGraph_t g)
+{
+    if (!x->l2win.num_bytes) return;
+    size_t n = 0;
+    if (cudaGraphGetNodes(g, nullptr, &n) != cudaSuccess || n == 0) return;
+    std::vector<cudaGraphNode_t> nodes(n);
+    if (cudaGraphGetNodes(g, nodes.data(), &n) != cudaSuccess) return;
+    cudaKernelNodeAttrValue v = {};
+    v.accessPolicyWindow = x->l2win;
+    for (cudaGraphNode_t nd : nodes) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel)
+            cudaGraphKernelNodeSetAttribute(nd, cudaKernelNodeAttributeAccessPolicyWindow, &v);
+    }
+    cudaGetLastError();
+}
+
 // Captures GRAPH_SIZES[gi] iterations into a graph starting at the current DPLUR buffer parity.
 static int build_graph(csu_ctx* x, int gi)
 {
@@ -1130,6 +1187,7 @@ static int build_graph(csu_ctx* x, int gi)
     for (int i = 0; i < GRAPH_SIZES[gi]; i++) DISPATCH(launch_iteration, x);
     cudaError_t e = cudaStreamEndCapture(x->stream, &g);
     if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+    apply_l2_window(x, g);
     e = cudaGraphInstantiate(&x->graphs[gi][q], g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
@@ -1733,11 +1791,22 @@ extern "C" int csu_time_kernels(csu_ctx* x, int iters, double* ms, int* count)
         if ((st = run_iterations(x, 1, 0, &h, nullptr))) return st;
     }
     CK(cudaStreamSynchronize(x->stream));
+    // the launches below are not graph nodes: give them the graphs' L2 window through the stream (the previous
+    // attribute of the caller's stream is put back afterwards)
+    cudaStreamAttrValue prev = {}, mine = {};
+    const bool win = x->l2win.num_bytes > 0 &&
+                     cudaStreamGetAttribute(x->stream, cudaStreamAttributeAccessPolicyWindow, &prev) == cudaSuccess;
+    if (win) {
+        mine.accessPolicyWindow = x->l2win;
+        CK(cudaStreamSetAttribute(x->stream, cudaStreamAttributeAccessPolicyWindow, &mine));
+    }
     x->timing = true;
     x->ev_used = 0;
     tmark(x, -1);
     for (int i = 0; i < iters; i++) DISPATCH(launch_iteration, x);
     x->timing = false;
+    if ((st = check_launch("timed iterations"))) return st;
+    if (win) CK(cudaStreamSetAttribute(x->stream, cudaStreamAttributeAccessPolicyWindow, &prev));
     if ((st = check_launch("timed iterations"))) return st;
     CK(cudaStreamSynchronize(x->stream));
     for (size_t i = 1; i < x->ev_used; i++) {

@@ -150,12 +150,13 @@ def test_sst_dplur_first_increment(native):
 
 
 def test_sst_dplur_fp32_runs(native):
-    """The extension with FP32 blocks and local steps moves the residual down on the SST plate."""
+    """The extension with FP32 blocks and local steps runs on the SST plate: the residual stays finite and
+    comes down from the peak of its start-up transient (the free-stream start has a residual near zero)."""
     import csu_b200
     wd = casekit.materialize("caseBL_turb", dict(KV, timeScheme="DPLUR", Nlinear="8", CFL="4.0",
                                                  implicitFP32="1", implicitLocalDt="1"))
     eng = csu_b200.Engine(csu_b200.Case.load(wd))
     h = eng.iterate(300)
     assert np.isfinite(h).all()
-    assert h[-1, 0] < h[0, 0]
+    assert h[-1, 0] < 0.5 * h[:, 0].max()
     eng.close()
