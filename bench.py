@@ -302,6 +302,8 @@ def main():
         dist.barrier()
     value = job_throughput(nc, args.steps, world, ms)
 
+    # the launch shapes the autotuner chose for this mesh (faces per flux block, cells per sweep block)
+    shapes = eng.autotune()
     # per-kernel device times of a few iterations, for the roofline of the dominant kernel
     kt = eng.time_kernels(5)
     names = ["prim", "grad", "flux", "rk", "impl", "sweep", "finalize", "resid", "blocks"]
@@ -360,7 +362,8 @@ def main():
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": workload_config(nc, case.n_faces, world),
-                "working_set_mb": ws_mb,
+                "working_set_mb": ws_mb, "launch_shapes": {"flux_faces_per_block": shapes[0],
+                                                           "sweep_cells_per_block": shapes[1]},
                 "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
                              "alg_bytes_per_launch": ab[dom], "ms_per_launch": per[dom]},

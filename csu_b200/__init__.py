@@ -48,7 +48,8 @@ class Config(C.Structure):
         ("inlet_t", C.c_double), ("sst_l", C.c_double), ("k_factor", C.c_double), ("o_factor", C.c_double),
         ("o_wall_factor", C.c_double), ("implicit_fp32", C.c_int), ("implicit_local_dt", C.c_int),
         ("cfl_ramp_iters", C.c_int), ("cfl_max", C.c_double), ("conv_drop", C.c_double),
-                ("iter_cap", C.c_int), ("limiter_func", C.c_int), ("gradient", C.c_int)]
+                ("iter_cap", C.c_int), ("limiter_func", C.c_int), ("gradient", C.c_int),
+                ("sa_implicit_source", C.c_int)]
 
 
 class MeshDesc(C.Structure):

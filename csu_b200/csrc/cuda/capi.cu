@@ -89,9 +89,10 @@ const double RK5[5] = {0.0533, 0.1263, 0.2375, 0.4414, 1.0};
 
 } // namespace
 
-// Launch shapes the autotuner chooses among (csu_autotune): faces per k_flux block and cells per DPLUR sweep
-// block. Neither changes a result bit: fluxes are per face, sweeps per cell, and the first sweep's partial
-// norms come one row per warp whatever the block size.
+// Launch shapes the autotuner chooses among (csu_autotune): faces per k_flux block (32 or 64 reading the
+// cells from global memory; 128 staging each block's cells through shared memory, k_flux_st) and cells per
+// DPLUR sweep block. None changes a result bit: fluxes are per face with the same arithmetic, sweeps per
+// cell, and the first sweep's partial norms come one row per warp whatever the block size.
 static const int FLUX_BLOCKS[3] = {32, 64, 128};
 static const int SWEEP_BLOCKS[3] = {64, 128, 256};
 
@@ -303,7 +304,9 @@ static void plan(csu_ctx* x, Arena& a)
     x->d_prm = carve<Prm>(a, x->nsolve);
     s.dbg_ghost = carve<double>(a, (size_t)(nb > 0 ? nb : 1) * (nv + 1));
     s.lsq_x87 = carve<unsigned long long>(a, 1);
-    s.dQ = x->cfg.sst && x->cfg.time_scheme != CSU_TS_RK ? carve<double>(a, (size_t)6 * nc) : nullptr;
+    s.dQ = x->cfg.sst && x->cfg.time_scheme != CSU_TS_RK ? carve<double>(a, (size_t)6 * nc)
+           : (x->cfg.sa && x->cfg.time_scheme == CSU_TS_DPLUR && x->cfg.sa_implicit_source) ? carve<double>(a, nc)
+                                                                                            : nullptr;
     s.gfix = carve<int2>(a, (size_t)nc * (nv + 1)); // at most one entry per cell and variable (and T)
     s.gfix_n = carve<unsigned>(a, 2);
     if (!x->is_pack) {
@@ -483,6 +486,7 @@ static void fill_params_from(const csu_config& c, const csu_layout& L, Prm& p)
     p.lim_func = c.limiter_func;
     if (c.gradient == 1) p.lsq_exact = 0; // Green-Gauss weights replace the least-squares weights
     p.blk32 = c.implicit_fp32;
+    p.sa_isrc = c.sa && c.time_scheme == CSU_TS_DPLUR && c.sa_implicit_source;
     p.implicit_local_dt = c.implicit_local_dt;
     p.cfl_ramp_iters = c.cfl_ramp_iters;
     p.cfl_max = c.cfl_ramp_iters > 0 ? c.cfl_max : c.cfl;
@@ -905,12 +909,21 @@ static void launch_flux_fb(csu_ctx* x, int coef)
     k_flux<MODEL, FB><<<gi + gb, FB, 0, x->stream>>>(x->d_prm, x->mesh, x->st, gi, x->d_wall_rank, coef);
 }
 
+// blocks of 128 faces whose cells are staged through a 256-cell shared-memory window (k_flux_st)
+template <int MODEL>
+static void launch_flux_staged(csu_ctx* x, int coef)
+{
+    constexpr int FB = 128;
+    const int gi = (x->L.nf + FB - 1) / FB, gb = (x->L.nb + FB - 1) / FB;
+    k_flux_st<MODEL, FB, 256><<<gi + gb, FB, 0, x->stream>>>(x->d_prm, x->mesh, x->st, gi, x->d_wall_rank, coef);
+}
+
 template <int MODEL>
 static void launch_flux(csu_ctx* x, int coef)
 {
     switch (x->flux_fb) {
     case 32: launch_flux_fb<MODEL, 32>(x, coef); break;
-    case 128: launch_flux_fb<MODEL, 128>(x, coef); break;
+    case 128: launch_flux_staged<MODEL>(x, coef); break;
     default: launch_flux_fb<MODEL, 64>(x, coef); break;
     }
     x->launches++;
@@ -1835,6 +1848,7 @@ struct csu_prep {
 // length may differ per solve.
 static bool same_structure(const csu_config& a, const csu_config& b)
 {
+    if (a.sa_implicit_source != b.sa_implicit_source) return false;
     return a.nvar == b.nvar && a.order == b.order && a.flux == b.flux && a.stages == b.stages &&
            a.time_scheme == b.time_scheme && a.n_linear == b.n_linear && a.dt_local == b.dt_local &&
            a.dt_local_n == b.dt_local_n && a.laminar == b.laminar && a.sa == b.sa && a.sa_cc == b.sa_cc &&

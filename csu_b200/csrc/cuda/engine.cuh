@@ -46,6 +46,7 @@ struct Prm {
     int blk0, nblk;     // its cell blocks (residual-norm partial sums)
     int wall0, nwall;   // its wall faces in the wall-coefficient array
     int blk32;          // DPLUR blocks in FP32
+    int sa_isrc;        // SA + DPLUR: the source's implicit part in the nt diagonal (dQ holds it per cell)
     int implicit_local_dt;
     int cfl_ramp_iters; // CFL ramp (0: constant CFL)
     double cfl_max;

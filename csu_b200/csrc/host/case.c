@@ -343,6 +343,7 @@ static int setup(csu_case* cs, const char* mesh_text, size_t mesh_len, const cha
     c->iter_cap = kw_int(kw, "iterCap", 0);
     c->limiter_func = kw_int(kw, "limiterFunc", 0);
     c->gradient = kw_int(kw, "gradient", 0);
+    c->sa_implicit_source = kw_int(kw, "saImplicitSource", 0);
 
     if (c->sa == 1 || c->sst == 1) csu_mesh_wall_distance(&cs->mesh);
 

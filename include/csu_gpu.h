@@ -88,6 +88,9 @@ typedef struct csu_config {
     int iter_cap;            /* packs: freeze a solve after this many iterations (iterCap; 0: none)     */
     int limiter_func;        /* limiterFunc: 0 Venkatakrishnan (reference), 1 Barth-Jespersen / minmod  */
     int gradient;            /* gradient: 0 least squares (reference), 1 Green-Gauss                    */
+    int sa_implicit_source;  /* saImplicitSource: SA with DPLUR, the source's destruction-dominated part in
+                                the diagonal of the nt row (-Omega min(dQ/d(rho nt), 0)); 0 explicit source
+                                as the reference                                                          */
 } csu_config;
 
 /*
@@ -257,7 +260,8 @@ int csu_time_kernels(csu_ctx* ctx, int iters, double* ms, int* count);
 int csu_residual_norms_noalloc(const double* R, int nvar, int ncells, double* res, void* stream);
 
 /* Launch-shape autotuner (no counterpart in the reference): times the face-chunk size of the face-flux
- * kernel (32, 64 or 128 faces per block) and the cell-block size of the DPLUR sweeps (64, 128 or 256) on this
+ * kernel (32 or 64 faces per block reading their cells from global memory, or 128 faces per block staging
+ * their cells through a shared-memory window) and the cell-block size of the DPLUR sweeps (64, 128 or 256) on this
  * context and keeps the fastest; neither choice changes a result bit. A context tunes itself on its first
  * csu_iterate (16,384 cells or more; a cache per device, model and size class spares packs of a class seen
  * before the timing); this call re-times now and reports the choice. CSU_AUTOTUNE=0 in the environment
