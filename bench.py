@@ -219,6 +219,21 @@ def serve_summary(n, cells_hi, rate):
             "workload": out["workload"], "wall_s": time.perf_counter() - t0}
 
 
+def airfoil_arm(args):
+    """Batched transonic SST airfoils (csu_b200.airfoilbench): one pack of many C-meshes, FP32 DPLUR blocks
+    against FP64 blocks, per-instance Cl/Cd differences."""
+    import torch
+    torch.cuda.set_device(0)
+    from csu_b200 import airfoilbench
+    out = airfoilbench.run(n=args.instances, ncells=args.instance_cells, iters=args.steps)
+    line = {"metric": "cell-updates/s", "value": out["fp32"]["cell_updates_per_s"], "unit": "cell-updates/s",
+            "n_gpus": 1, "steps": args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64 residual, f32 DPLUR blocks", "data": "synthetic",
+            "config": dict(out["workload"], workload="batched SST airfoils"), "result": out}
+    print(json.dumps(line))
+    return 0
+
+
 def serve_arm(args):
     """Serving stream (csu_b200.servebench): requests of four geometry families arriving as a Poisson stream,
     served by the continuous-batching server (packs, FP32 DPLUR blocks) and by the plain FP64 path one solve
@@ -251,11 +266,17 @@ def main():
     ap.add_argument("--requests", type=int, default=40)
     ap.add_argument("--cells-hi", type=float, default=2e5)
     ap.add_argument("--rate", type=float, default=5.0, help="serving stream: Poisson arrivals per second")
+    ap.add_argument("--airfoils", action="store_true",
+                    help="the batched SST airfoil pack instead (FP32 vs FP64 DPLUR blocks, Cl/Cd differences)")
+    ap.add_argument("--instances", type=int, default=64)
+    ap.add_argument("--instance-cells", type=int, default=65536)
     ap.add_argument("--no-serve", action="store_true",
                     help="leave the bounded serving comparison out of the default line")
     args = ap.parse_args()
     if args.serve:
         return serve_arm(args)
+    if args.airfoils:
+        return airfoil_arm(args)
     args.warmup = max(args.warmup, 3)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -38,6 +38,11 @@ __device__ __forceinline__ double sa_source(double ni, double ni_L, double S, do
     double cv3 = 0.9;
     if (Sbar >= -cv2 * S) Stil = S + Sbar;
     else Stil = S + S * (cv2 * cv2 * S + cv3 * Sbar) / ((cv3 - 2 * cv2) * S - Sbar);
+    // In exact arithmetic this modified vorticity is at least 0.3 S >= 0; with a denormal S (a uniform free
+    // stream) the rounded product S * (...) can exceed S and leave it negative, and then r = -inf and fw is
+    // NaN, in the reference's expression as here. A negative value is therefore taken as +0 (r -> 10, as any
+    // tiny positive value gives); wherever the reference's result is finite nothing changes.
+    if (Stil < 0.0) Stil = 0.0;
     double sig = 2. / 3.;
     double Cb1 = 0.1355;
     double Cb2 = 0.622;

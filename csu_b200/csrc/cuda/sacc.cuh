@@ -44,6 +44,8 @@ __device__ __forceinline__ double sacc_source(double ni, double ni_L, double S, 
         if (aux2 == 0) Stil = S;
         else Stil = S + S * (cv2 * cv2 * S + cv3 * Sbar) / aux2;
     }
+    // as in sa_source: a negative value, reachable only by rounding a denormal S, is taken as +0
+    if (Stil < 0.0) Stil = 0.0;
     double sig = 2. / 3.;
     double Cb1 = 0.1355;
     double Cb2 = 0.622;

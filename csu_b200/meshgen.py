@@ -104,6 +104,8 @@ def _solver_kv(flux="AUSMDV", order=1, scheme="DPLUR", n_linear=4, cfl=5.0, nmax
     elif viscous == "sa":
         kv["sa"] = "1"
         kv["turbRatio"] = "3"
+    elif viscous == "sst":
+        kv["sst"] = "1"
     return kv
 
 

@@ -8,7 +8,7 @@ for bit on this mesh, and so is the residual except the SA variable's in about 7
 1 to 4 ulps: the SA destruction function's pow(x, 1/6) (saCalcSource, sa.c:343) rounds its last bit
 differently in CUDA's and glibc's libm. The DPLUR finite-difference blocks (h = 1e-6) amplify those bits
 over the iterations: the 100-iteration residual history agrees to 2e-7 relative (measured 9.5e-8), the
-state to 1e-8 of each variable's scale (measured 6e-10 on the mean flow, 6e-7 of nt's scale). The first
+state to 1e-8 of each variable's scale (measured 9e-10, the momentum components on the momentum's scale). The first
 10 iterations are the reference's bit for bit apart from the reported state's write-back clamp timing."""
 import numpy as np
 import pytest
@@ -38,7 +38,10 @@ def test_sa_plate_full_size_100_iterations(native):
     rel = np.max(np.abs(h[:, :nv] - h_ref[:, :nv]) / np.abs(h_ref[:, :nv]))
     assert rel < 2e-7, rel
     U, U_ref = eng.get_state(), ref.get_U()
+    # scales: each variable's largest magnitude, the momentum components both by the momentum's (rho v is
+    # nearly zero on a flat plate)
     us = np.abs(U_ref).max(axis=1, keepdims=True)
+    us[1:3] = max(us[1, 0], us[2, 0])
     du = np.max(np.abs(U - U_ref) / us, axis=1)
-    assert du[:4].max() < 1e-8 and du[4] < 1e-5, du
+    assert du.max() < 1e-8, du
     eng.close()
