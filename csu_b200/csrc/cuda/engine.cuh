@@ -39,7 +39,7 @@ struct Prm {
     double sst_b1, o_wall_factor;
     SstK sst_k;         // SST constants (sstInit)
     double tmax;        // tube end time
-    double conv_tol;    // stop when res[0] <= conv_tol * res0[0] (0: never)
+    double conv_tol;    // stop when res[0] <= conv_tol * res0[0], res0 the largest residual so far (0: never)
     int iter_cap;       // freeze the solve (done = 2) once its counter reaches this (0: never)
     int lim_func;       // limiter function: 0 Venkatakrishnan (limiterV2), 1 Barth-Jespersen (limiterBJ)
     int cell0;          // first cell of this solve (packs: cells [cell0, cell0 + nc), block aligned)

@@ -1699,11 +1699,17 @@ __global__ void __launch_bounds__(BLOCK) k_finalize(const Prm* __restrict__ P, c
             row[NV] = cxp; row[NV + 1] = cxv; row[NV + 2] = cyp; row[NV + 3] = cyv;
         }
         sc->hist_row = S.hist_row + 1;
+        // the residual-drop stop measures from the largest residual so far (a free-stream start has a first
+        // density residual of round-off size; the start-up transient then raises it)
         double r00 = S.res0[0];
         if (!S.have_res0) {
             for (int k = 0; k < NV; k++) sc->res0[k] = res[k];
             sc->have_res0 = 1;
             r00 = res[0];
+        } else {
+            for (int k = 0; k < NV; k++)
+                if (res[k] > S.res0[k]) sc->res0[k] = res[k];
+            r00 = fmax(r00, res[0]);
         }
         sc->steps = S.steps + 1;
         if (S.iter == p.dt_local_n) sc->dt_local = 0;

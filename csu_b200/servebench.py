@@ -11,7 +11,8 @@ inflow); half laminar with Re log-uniform in [1e3, 1e5], half Spalart-Allmaras w
 [1e6, 1e7]; Poisson arrivals at `rate` per second; all from numpy default_rng(seed).
 
 Solver settings, the same in both arms: first order, AUSM, DPLUR with 16 sweeps and local time steps at
-CFL 16, stop at a residual drop `drop` of the RMS density residual or after `max_iters` iterations. AUSM
+CFL 16, stop at a residual drop `drop` of the RMS density residual (from its largest value so far) or after
+`max_iters` iterations. AUSM
 rather than AUSMDV: AUSMDV's switches leave the reference's own solution limit-cycling at 1e-5..1e-4 of the
 initial residual on the cylinder (its LU-SGS at CFL 1000 as well), so no 1e-8 drop exists for it to reach;
 AUSM converges the same case to 1e-13. The airfoil family is left out of the default stream: on its C-mesh

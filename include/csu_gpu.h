@@ -84,7 +84,7 @@ typedef struct csu_config {
     int cfl_ramp_iters;      /* CFL grows geometrically from CFL to cfl_max over this many iterations
                                 (keywords CFLramp, CFLmax)                                              */
     double cfl_max;
-    double conv_drop;        /* stop once res[0] <= conv_drop * res[0] of the first iteration (convDrop) */
+    double conv_drop;        /* stop once res[0] <= conv_drop * the largest res[0] so far (convDrop)     */
     int iter_cap;            /* packs: freeze a solve after this many iterations (iterCap; 0: none)     */
     int limiter_func;        /* limiterFunc: 0 Venkatakrishnan (reference), 1 Barth-Jespersen / minmod  */
     int gradient;            /* gradient: 0 least squares (reference), 1 Green-Gauss                    */
@@ -289,8 +289,8 @@ typedef struct csu_solve_info {
     int done;        /* 1: the residual-drop stop (convDrop) was reached; 2: iterCap; 3: stopped by
                         csu_pack_stop                                                */
     int hist_rows;   /* history rows recorded by the last csu_iterate call          */
-    int have_res0;   /* res0 holds the first residual                              */
-    double res0[6];  /* RMS residuals of the solve's first iteration               */
+    int have_res0;   /* res0 holds a residual                                       */
+    double res0[6];  /* largest RMS residuals of the solve so far (per variable)    */
     double res[6];   /* RMS residuals of its last iteration                         */
     double coef[4];  /* Cx_p, Cx_v, Cy_p, Cy_v of its last iteration                */
 } csu_solve_info;

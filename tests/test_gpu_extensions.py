@@ -93,8 +93,10 @@ def test_conv_drop_stops_at_threshold(native):
     hist = eng.iterate_until(N_ITER)
     n = len(hist)
     assert 1 < n < N_ITER
-    assert hist[-1, 0] <= 1e-6 * hist[0, 0]
-    assert np.all(hist[:-1, 0] > 1e-6 * hist[0, 0])
+    # the drop is measured from the largest residual so far
+    peak = np.maximum.accumulate(hist[:, 0])
+    assert hist[-1, 0] <= 1e-6 * peak[-1]
+    assert np.all(hist[:-1, 0] > 1e-6 * peak[:-1])
     # the state left behind is the one after the last reported iteration: continuing matches a plain run
     U = eng.get_state()
     eng.close()

@@ -41,8 +41,9 @@ def test_plate_sa_roe_configuration_runs(native):
     eng = csu_b200.Engine(case)
     h = eng.iterate(600)
     U = eng.get_state()
-    print("\nplate SA (Roe, Barth-Jespersen, FP32 DPLUR, CFL ramp): rho residual %.3e -> %.3e"
-          % (h[0, 0], h[-1, 0]))
+    print("\nplate SA (Roe, Barth-Jespersen, FP32 DPLUR, CFL ramp): rho residual peak %.3e -> %.3e"
+          % (h[:, 0].max(), h[-1, 0]))
     assert np.all(np.isfinite(U))
-    assert h[-1, 0] < 2e-2 * h[0, 0]
+    # the free-stream start has a density residual of round-off size: the drop is from the transient's peak
+    assert h[-1, 0] < 2e-2 * h[:, 0].max()
     eng.close()
