@@ -5,8 +5,8 @@ for 65,536 cells by default, first cell 1e-6 chord, far field at 100 chords; csu
 with its own Mach number M ~ U[0.5, 0.85] and angle of attack alpha ~ U[-4, 4] deg from numpy
 default_rng(seed), Re = 6e6 on the chord, Menter SST. All solves form one pack (csu_pack_*): every kernel
 of an iteration is one launch for all of them, replayed from CUDA graphs. Solver settings: first order, AUSM,
-DPLUR with local time steps (an extension: the reference's SST DPLUR is undefined), the SST k-omega source
-block in the diagonal, CFL ramped geometrically from `cfl0` to `cfl1` over `ramp` iterations.
+DPLUR with local time steps (an extension: the reference's SST DPLUR is undefined), the destruction part of
+the SST source Jacobians in the diagonal, CFL ramped geometrically from `cfl0` to `cfl1` over `ramp` iterations.
 
 Two packs of the same solves run the same number of iterations: FP64 blocks and FP32 blocks (the residual,
 the state and the sweeps' accumulation stay FP64 in both). Reported: per-instance lift and drag coefficients

@@ -1188,8 +1188,11 @@ __global__ void __launch_bounds__(BLOCK, 3) k_blocks(const Prm* __restrict__ P, 
     double A[NV * NV];
 #pragma unroll
     for (int mm = 0; mm < NV; mm++) {
+        // SST: rho omega reaches 1e10 beside a wall, where a step of 1e-6 is below its last bit; its column
+        // (a flux linear in rho omega) takes a step relative to the value
+        const double hm = MODEL == 2 && mm >= 4 ? h * fmax(1.0, fabs(Un[mm])) : h;
 #pragma unroll
-        for (int nn = 0; nn < NV; nn++) Uq[nn] = mm == nn ? Un[nn] + h : Un[nn];
+        for (int nn = 0; nn < NV; nn++) Uq[nn] = mm == nn ? Un[nn] + hm : Un[nn];
         double r2 = Uq[0];
         double u2 = Uq[1] / r2;
         double v2 = Uq[2] / r2;
@@ -1200,7 +1203,7 @@ __global__ void __launch_bounds__(BLOCK, 3) k_blocks(const Prm* __restrict__ P, 
         double pr = p.gas.R * r2 * T;
         aux_flux<NV>(Uq, pr, nx, ny, F);
 #pragma unroll
-        for (int nn = 0; nn < NV; nn++) A[nn * NV + mm] = 0.5 * (F[nn] - F0[nn]) * dS / h;
+        for (int nn = 0; nn < NV; nn++) A[nn * NV + mm] = 0.5 * (F[nn] - F0[nn]) * dS / hm;
     }
     double cc = T2c(p.gas, Pn[4]);
     double ra = p.w_imp * (fabs(nx * Pn[1] + ny * Pn[2]) + cc) * dS;
@@ -1339,25 +1342,20 @@ __global__ void __launch_bounds__(SB) k_sweep(const Prm* __restrict__ P, const _
             }
             const double w = 2. / 3.;
             if constexpr (MODEL == 2) {
-                // SST (extension): the diagonal block is D on the mean flow and, on k and omega, D minus the
-                // source Jacobians (the 2x2 block of the LU-SGS diagonal, implicit.c:323-345, with its
-                // coupling to rho): x* = Dblock^-1 (-R - sum_j A_j x_j), then x += w (x* - x)
+                // SST (extension): D on the mean flow; on k and omega, D minus the non-positive (destruction)
+                // part of the source Jacobians' diagonal, with their coupling to rho (the LU-SGS diagonal
+                // block, implicit.c:323-345, without its production part and k-omega cross terms, which made
+                // the iteration diverge at CFL 2 on wall-resolved meshes): x* = Dblock^-1 (-R - sum_j A_j x_j),
+                // then x += w (x* - x)
                 double z[NV], xs[NV];
 #pragma unroll
                 for (int k = 0; k < NV; k++) z[k] = -R[k] - y[k];
 #pragma unroll
                 for (int k = 0; k < 4; k++) xs[k] = z[k] / D;
-                const double a = D - s.dQ[(size_t)nc + c], b = -s.dQ[(size_t)2 * nc + c];
-                const double cq = -s.dQ[(size_t)4 * nc + c], dq = D - s.dQ[(size_t)5 * nc + c];
-                const double Ak = z[4] + s.dQ[c] * xs[0], Bw = z[5] + s.dQ[(size_t)3 * nc + c] * xs[0];
-                const double det = a * dq - b * cq;
-                if (fabs(det) < 1e-14) {
-                    xs[4] = z[4] / D;
-                    xs[5] = z[5] / D;
-                } else {
-                    xs[4] = (Ak * dq - Bw * b) / det;
-                    xs[5] = (-Ak * cq + Bw * a) / det;
-                }
+                const double a = D - fmin(s.dQ[(size_t)nc + c], 0.0);
+                const double dq = D - fmin(s.dQ[(size_t)5 * nc + c], 0.0);
+                xs[4] = (z[4] + s.dQ[c] * xs[0]) / a;
+                xs[5] = (z[5] + s.dQ[(size_t)3 * nc + c] * xs[0]) / dq;
 #pragma unroll
                 for (int k = 0; k < NV; k++) xn[k] = xo[k] + w * (xs[k] - xo[k]);
             } else {
