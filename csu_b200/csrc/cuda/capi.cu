@@ -142,6 +142,12 @@ struct csu_ctx {
     // DPLUR blocks run on a side stream, forked from and joined back to the engine stream
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    // DPLUR graph capture: iterations in the graph being captured and the next one's index; an iteration's
+    // k_finalize left to run on the side stream beside the next iteration's gradients and fluxes, with the
+    // face-coefficient buffer it sums
+    int defer_n = 0, defer_i = 0;
+    bool fin_pending = false;
+    int fin_bsel = 0;
     int max_ni = 4;          // most interior faces of a cell (k_blocks covers slots [0, max_ni))
     int flux_fb = 64;        // faces per k_flux block (one of FLUX_BLOCKS)
     int sweep_sb = 128;      // cells per DPLUR sweep block (one of SWEEP_BLOCKS)
@@ -298,6 +304,7 @@ static void plan(csu_ctx* x, Arena& a)
     // partial norms: one row per 256-cell block, or per 128-cell block from the DPLUR first sweep
     s.part = carve<double>(a, (size_t)((nc + BLOCK - 1) / BLOCK) * (BLOCK / 32) * nv);
     s.bcoef = carve<double>(a, (size_t)4 * (nb > 0 ? nb : 1));
+    s.bcoef2 = dplur ? carve<double>(a, (size_t)4 * (nb > 0 ? nb : 1)) : nullptr;
     s.sc = carve<Scalars>(a, x->nsolve);
     s.bsolve = x->nsolve > 1 ? carve<int>(a, (nc + BLOCK - 1) / BLOCK) : nullptr;
     s.csolve = x->nsolve > 1 ? carve<int>(a, nc) : nullptr;
@@ -487,6 +494,7 @@ static void fill_params_from(const csu_config& c, const csu_layout& L, Prm& p)
     if (c.gradient == 1) p.lsq_exact = 0; // Green-Gauss weights replace the least-squares weights
     p.blk32 = c.implicit_fp32;
     p.sa_isrc = c.sa && c.time_scheme == CSU_TS_DPLUR && c.sa_implicit_source;
+    p.defer_fin = c.time_scheme == CSU_TS_DPLUR;
     p.implicit_local_dt = c.implicit_local_dt;
     p.cfl_ramp_iters = c.cfl_ramp_iters;
     p.cfl_max = c.cfl_ramp_iters > 0 ? c.cfl_max : c.cfl;
@@ -931,11 +939,12 @@ static void launch_flux(csu_ctx* x, int coef)
 }
 
 template <int MODEL>
-static void launch_finalize(csu_ctx* x, int mode)
+static void launch_finalize(csu_ctx* x, int mode, int bsel = 0, cudaStream_t stream = nullptr)
 {
     // the first DPLUR sweep writes one partial row per warp; the other kernels one per cell block
     const int ppb = x->cfg.time_scheme == CSU_TS_DPLUR && mode == 1 ? BLOCK / 32 : 1;
-    k_finalize<MODEL><<<x->nsolve, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st, mode, ppb);
+    k_finalize<MODEL><<<x->nsolve, BLOCK, 0, stream ? stream : x->stream>>>(x->d_prm, x->mesh, x->st, mode, ppb,
+                                                                            bsel);
     x->launches++;
     tmark(x, KFIN);
 }
@@ -966,6 +975,12 @@ static void launch_blocks(csu_ctx* x)
     k_blocks<MODEL><<<x->max_ni * x->gb_c, BLOCK, 0, s>>>(x->d_prm, x->mesh, x->st, x->gb_c);
     x->launches++;
     if (x->timing) tmark(x, KBLK);
+    if (x->fin_pending) {
+        // the previous iteration's k_finalize, after the blocks (which need no scalar it writes) and before
+        // the diagonal (whose step minimum it resets)
+        launch_finalize<MODEL>(x, 1, x->fin_bsel, s);
+        x->fin_pending = false;
+    }
     k_impl<MODEL, false><<<x->gb_c, BLOCK, 0, s>>>(x->d_prm, x->mesh, x->st);
     x->launches++;
     if (x->timing) tmark(x, KIMPL);
@@ -1066,11 +1081,23 @@ static void launch_iteration(csu_ctx* x)
         // gradients, for its source Jacobians); the Euler/laminar ones only the iteration's start state
         constexpr bool early = MODEL == 0;
         const bool grad = c.order == 2 || x->prm.visc;
+        // Inside a captured graph an iteration's k_finalize (norms, history row, halt flags, counters) runs on
+        // the side stream beside the next iteration's gradients and face fluxes, which test halted_behind;
+        // the graph's last iteration finalizes in line. The face coefficients alternate between two buffers,
+        // so that the next k_flux does not overwrite the ones being summed.
+        const bool defer = x->defer_n > 0 && !x->timing;
+        const int bsel = defer ? (x->defer_i & 1) : 0;
         if (!x->timing) cudaEventRecord(x->ev_fork, x->stream);
+        if (x->fin_pending && !early) {
+            // the side stream waits for k_flux before the blocks: the pending k_finalize goes first
+            cudaStreamWaitEvent(x->side, x->ev_fork, 0);
+            launch_finalize<MODEL>(x, 1, x->fin_bsel, x->side);
+            x->fin_pending = false;
+        }
         if (grad) launch_grad<MODEL>(x, false);
         snapshot_views(x);
         if (early) launch_blocks<MODEL>(x);
-        launch_flux<MODEL>(x, 1);
+        launch_flux<MODEL>(x, 1 + bsel);
         if (!early) {
             if (!x->timing) cudaEventRecord(x->ev_fork, x->stream);
             launch_blocks<MODEL>(x);
@@ -1078,7 +1105,13 @@ static void launch_iteration(csu_ctx* x)
         if (!x->timing) cudaStreamWaitEvent(x->stream, x->ev_join, 0);
         // the first sweep gathers R (and its norms) from the face fluxes
         for (int m = 0; m < c.n_linear; m++) launch_sweep<MODEL>(x, m, c.n_linear);
-        launch_finalize<MODEL>(x, 1);
+        if (defer && x->defer_i + 1 < x->defer_n) {
+            x->fin_pending = true;
+            x->fin_bsel = bsel;
+        } else {
+            launch_finalize<MODEL>(x, 1, bsel);
+        }
+        if (defer) x->defer_i++;
     }
 }
 
@@ -1197,7 +1230,11 @@ static int build_graph(csu_ctx* x, int gi)
     long long l0 = x->launches;
     cudaGraph_t g;
     CK(cudaStreamBeginCapture(x->stream, cudaStreamCaptureModeThreadLocal));
+    x->defer_n = GRAPH_SIZES[gi];
+    x->defer_i = 0;
+    x->fin_pending = false;
     for (int i = 0; i < GRAPH_SIZES[gi]; i++) DISPATCH(launch_iteration, x);
+    x->defer_n = 0;
     cudaError_t e = cudaStreamEndCapture(x->stream, &g);
     if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
     apply_l2_window(x, g);
@@ -1376,6 +1413,8 @@ __global__ void k_call_begin(Scalars* sc, int n, int it0, int set_iter)
     sc[k].hist_row = 0;
     sc[k].steps = 0;
     if (set_iter) sc[k].iter = it0;
+    // halt flags set or cleared between calls take effect for every kernel from the call's first launch
+    sc[k].frozen = (sc[k].status | sc[k].done) != 0;
 }
 
 // The parity the DPLUR increment buffers have after `iters` iterations from parity q.
@@ -1614,6 +1653,7 @@ extern "C" int csu_residual(csu_ctx* x, double* R)
     if ((st = read_scalars(x, &h))) return st;
     h.done = 0;
     h.status = 0;
+    h.frozen = 0;
     if ((st = write_scalars_n(x, &h, 1))) return st;
     DISPATCH(launch_residual, x, true);
     if ((st = check_launch("residual"))) return st;

@@ -47,6 +47,7 @@ struct Prm {
     int wall0, nwall;   // its wall faces in the wall-coefficient array
     int blk32;          // DPLUR blocks in FP32
     int sa_isrc;        // SA + DPLUR: the source's implicit part in the nt diagonal (dQ holds it per cell)
+    int defer_fin;      // DPLUR: an iteration's k_finalize may run beside the next one's gradients and fluxes
     int implicit_local_dt;
     int cfl_ramp_iters; // CFL ramp (0: constant CFL)
     double cfl_max;
@@ -71,6 +72,9 @@ struct Scalars {
     int steps;                            // iterations completed in this call
     int have_res0;                        // res0 recorded
     int fresh;                            // state set from outside: the prologue derives W and the step
+    int frozen;                           // (status | done) as the last DPLUR k_finalize found them on entry, or
+                                          // as the call found them (k_call_begin): the halt test of the kernels
+                                          // that run beside a deferred k_finalize (halted_behind)
     int hist_cap;                         // rows available at hist
     double* hist;                         // history rows of this solve (or null)
 };
@@ -136,6 +140,8 @@ struct State {
     float* blocks32;                          // the same in FP32 (mixed-precision DPLUR)
     double* part;                             // per-block partial sums of R^2 [block][NV]
     double* bcoef;                            // per reference boundary face: cp dSx, cp dSy, fx/q, fy/q
+    double* bcoef2;                           // DPLUR: the second buffer (iterations alternate, so that a deferred
+                                              // k_finalize sums one while the next k_flux writes the other)
     Scalars* sc;                              // one per solve
     const int* bsolve;                        // packs: solve of each cell block (null: one solve)
     const int* csolve;                        // packs: solve of each cell (null: one solve)

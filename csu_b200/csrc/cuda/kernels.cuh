@@ -24,6 +24,16 @@ __device__ __forceinline__ bool halted(const Scalars* sc)
     return (sc->status | sc->done) != 0;
 }
 
+// The halt test of the kernels that, in DPLUR, may run beside the previous iteration's k_finalize (limiter
+// bounds, gradients, face fluxes): the flags k_finalize is writing are not read; `frozen` (the flags one
+// k_finalize behind) is. A solve halted by iteration i's k_finalize therefore still gets iteration i + 1's
+// gradients and face fluxes, of the state it stopped at, and nothing after them: its later iterations
+// either skip these kernels or recompute the same values, whichever flag value they read.
+__device__ __forceinline__ bool halted_behind(const Prm& p, const Scalars* sc)
+{
+    return p.defer_fin ? sc->frozen != 0 : halted(sc);
+}
+
 // Solve of a cell block (in a pack every block holds cells of one solve) and of a cell; cells of the
 // solve are [p.cell0, p.cell0 + p.nc), the rest of its last block is padding.
 __device__ __forceinline__ int block_solve(const State& s)
@@ -176,7 +186,7 @@ __global__ void __launch_bounds__(BLOCK) k_minmax(const Prm* __restrict__ P, con
     const int sid = block_solve(s);
     const Prm& p = P[sid];
     Scalars* const sc = s.sc + sid;
-    if (halted(sc)) return;
+    if (halted_behind(p, sc)) return;
     const int c = blockIdx.x * BLOCK + threadIdx.x;
     const bool ok = cell_in(p, c);
     double W[NP];
@@ -207,7 +217,7 @@ __global__ void __launch_bounds__(BLOCK, 3) k_grad(const Prm* __restrict__ P, co
     const Prm& p = P[sid];
     Scalars* const sc = s.sc + sid;
     const int c = blockIdx.x * BLOCK + threadIdx.x;
-    if (!cell_in(p, c) || halted(sc)) return;
+    if (!cell_in(p, c) || halted_behind(p, sc)) return;
     {
         const int nc = m.nc;
         double P0[NP];
@@ -675,7 +685,7 @@ __device__ __forceinline__ void boundary_face(const Prm* __restrict__ P, const M
     int c = m.bown[b];
     const int sid = cell_solve(s, c);
     const Prm& p = P[sid];
-    if (halted(s.sc + sid)) return;
+    if (halted_behind(p, s.sc + sid)) return;
     int flag = m.bflag[b];
     double2 dSv = m.bn[b];
     double dSx = dSv.x, dSy = dSv.y, dS = m.bds[b];
@@ -699,16 +709,17 @@ __device__ __forceinline__ void boundary_face(const Prm* __restrict__ P, const M
         bface_visc<MODEL>(p, m, s, b, fi, c, flag, dSx, dSy, E0, gvx, gvy, bdv, bLv);
     }
     if (coef && (flag == 3 || flag == 4)) {
+        double* const bc = coef == 2 ? s.bcoef2 : s.bcoef;
         double G[NP];
         ghost_state<MODEL>(p, flag, dSx, dSy, dS, E0, m.wall_d ? m.wall_d[c] : 0.0, G);
         double cp = (G[3] - p.p_inf) / p.q_inf;
         int r = wall_rank[b];
-        s.bcoef[(size_t)r * 4 + 0] = cp * dSx;
-        s.bcoef[(size_t)r * 4 + 1] = cp * dSy;
+        bc[(size_t)r * 4 + 0] = cp * dSx;
+        bc[(size_t)r * 4 + 1] = cp * dSy;
         double fx = 0.0, fy = 0.0;
         if (p.visc) friction_wall(gvx, gvy, E0, dSx, dSy, bdv.x, bdv.y, bLv, &fx, &fy);
-        s.bcoef[(size_t)r * 4 + 2] = p.visc ? fx / p.q_inf : 0.0;
-        s.bcoef[(size_t)r * 4 + 3] = p.visc ? fy / p.q_inf : 0.0;
+        bc[(size_t)r * 4 + 2] = p.visc ? fx / p.q_inf : 0.0;
+        bc[(size_t)r * 4 + 3] = p.visc ? fy / p.q_inf : 0.0;
     }
 }
 
@@ -729,7 +740,7 @@ __global__ void __launch_bounds__(FB) k_flux(const Prm* __restrict__ P, const __
         int2 e = m.fe[f];
         const int sid = cell_solve(s, e.x);
         const Prm& p = P[sid];
-        if (halted(s.sc + sid)) return;
+        if (halted_behind(p, s.sc + sid)) return;
         const double4 z4 = make_double4(0.0, 0.0, 0.0, 0.0);
         const bool grad = p.order == 2 || p.visc;
         interior_face<MODEL>(p, m, s, f, e, s.W4[e.x], s.WT[e.x], grad ? s.G4x[e.x] : z4, grad ? s.G4y[e.x] : z4,
@@ -786,7 +797,7 @@ __global__ void __launch_bounds__(FB) k_flux_st(const Prm* __restrict__ P, const
     const int2 e = m.fe[f];
     const int sid = cell_solve(s, e.x);
     const Prm& p = P[sid];
-    if (halted(s.sc + sid)) return;
+    if (halted_behind(p, s.sc + sid)) return;
     const double4 z4 = make_double4(0.0, 0.0, 0.0, 0.0);
     const unsigned i0 = (unsigned)(e.x - base), i1 = (unsigned)(e.y - base);
     const bool in0 = i0 < (unsigned)WIN, in1 = i1 < (unsigned)WIN;
@@ -1616,11 +1627,12 @@ __global__ void __launch_bounds__(BLOCK) k_update(const Prm* __restrict__ P, con
 // ------------------------------------------------------------------------------------------------
 // k_finalize: one block closing an iteration (solverCalcRes, solverCalcCoeff3, history row, flags) and
 // preparing the next step size. mode: 0 RK iteration, 1 implicit iteration, 2 prologue (step size only),
-// 3 residual only (norms).
+// 3 residual only (norms). bsel: the face-coefficient buffer k_flux wrote (0 bcoef, 1 bcoef2). In mode 1
+// it records the halt flags it found on entry in `frozen` (halted_behind).
 // ------------------------------------------------------------------------------------------------
 template <int MODEL>
 __global__ void __launch_bounds__(BLOCK) k_finalize(const Prm* __restrict__ P, const __grid_constant__ Mesh m,
-                                                    const __grid_constant__ State s, int mode, int ppb)
+                                                    const __grid_constant__ State s, int mode, int ppb, int bsel)
 {
     constexpr int NV = Model<MODEL>::NV;
     __shared__ double sh[NV + 4][BLOCK / 32];
@@ -1630,7 +1642,7 @@ __global__ void __launch_bounds__(BLOCK) k_finalize(const Prm* __restrict__ P, c
     // ppb rows of partial norms per cell block (the DPLUR first sweep writes one per 128 cells)
     const int npart = p.nblk * ppb, nwall = p.nwall;
     const double* part = s.part + (size_t)p.blk0 * ppb * NV;
-    const double* bcoef = s.bcoef + (size_t)p.wall0 * 4;
+    const double* bcoef = (bsel ? s.bcoef2 : s.bcoef) + (size_t)p.wall0 * 4;
     // Everything the block reads is requested before the halted test, so the loads overlap: a chain of
     // dependent round trips to the L2 would be most of a one-block kernel's time. Thread 0 keeps a copy of
     // the solve's scalars and writes back only what changes.
@@ -1670,7 +1682,10 @@ __global__ void __launch_bounds__(BLOCK) k_finalize(const Prm* __restrict__ P, c
         }
     }
     Scalars S;
-    if (threadIdx.x == 0) S = *sc;
+    if (threadIdx.x == 0) {
+        S = *sc;
+        if (mode == 1) sc->frozen = stop;
+    }
     if (stop) return;
     block_sum<NV + 4>(v, sh);
     if (threadIdx.x != 0) return;
