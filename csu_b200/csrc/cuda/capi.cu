@@ -765,6 +765,38 @@ __global__ void k_state_in(State s, const double* stage, const int* n2o, int nc,
     for (int r = 4; r < nv; r++) s.Ux[(size_t)(r - 4) * nc + c] = stage[(size_t)r * nc + q];
 }
 
+// DPLUR one-solve contexts: the state goes in with its primitives (U := clamp(U), W = primitives, as the
+// prologue's k_prim computes them) ...
+template <int MODEL>
+__global__ void __launch_bounds__(BLOCK) k_state_in_prim(const Prm* __restrict__ P, State s, const double* stage,
+                                                         const int* n2o, int nc)
+{
+    constexpr int NV = Model<MODEL>::NV, NP = Model<MODEL>::NP;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= nc) return;
+    const int q = n2o[c];
+    double U[NV], W[NP];
+#pragma unroll
+    for (int k = 0; k < NV; k++) U[k] = stage[(size_t)k * nc + q];
+    clamp_prim<MODEL>(P[0], U, W);
+    storeU<MODEL>(s, nc, c, U);
+    storeP<MODEL>(s, nc, c, W);
+}
+
+// ... and fresh scalars, as reset_scalars and the prologue's k_finalize leave them for DPLUR (the step
+// size the prologue computes is an RK quantity), so that the next call goes straight to its iterations
+__global__ void k_scalars_fresh(Scalars* sc, double* hist, int hist_cap, int dt_local)
+{
+    if (threadIdx.x != 0) return;
+    Scalars h;
+    memset(&h, 0, sizeof(h));
+    h.dtmin_bits = 0x7ff0000000000000ULL;
+    h.dt_local = dt_local;
+    h.hist = hist;
+    h.hist_cap = hist_cap;
+    *sc = h;
+}
+
 __global__ void k_state_out(State s, double* stage, const int* n2o, int nc, int nv)
 {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -787,10 +819,22 @@ static int solve_state_io(csu_ctx* x, int k, double* U, bool put)
         const int g = (nc + BLOCK - 1) / BLOCK;
         if (put) {
             CK(cudaMemcpyAsync(x->d_stage, U, bytes, cudaMemcpyHostToDevice, x->stream));
-            k_state_in<<<g, BLOCK, 0, x->stream>>>(x->st, x->d_stage, x->d_n2o, nc, nv);
+            const bool dplur = x->cfg.time_scheme == CSU_TS_DPLUR;
+            if (dplur) {
+                // primitives and fresh scalars on the device: the next csu_iterate needs no host round trip
+                // for the scalars and no prologue kernels
+                switch (x->model) {
+                case 0: k_state_in_prim<0><<<g, BLOCK, 0, x->stream>>>(x->d_prm, x->st, x->d_stage, x->d_n2o, nc); break;
+                case 1: k_state_in_prim<1><<<g, BLOCK, 0, x->stream>>>(x->d_prm, x->st, x->d_stage, x->d_n2o, nc); break;
+                default: k_state_in_prim<2><<<g, BLOCK, 0, x->stream>>>(x->d_prm, x->st, x->d_stage, x->d_n2o, nc); break;
+                }
+                k_scalars_fresh<<<1, 32, 0, x->stream>>>(x->st.sc, hist_of(x, 0), x->hist_cap, x->cfg.dt_local);
+            } else {
+                k_state_in<<<g, BLOCK, 0, x->stream>>>(x->st, x->d_stage, x->d_n2o, nc, nv);
+            }
             CK(cudaGetLastError());
             CK(cudaStreamSynchronize(x->stream)); // the caller may reuse U on return
-            x->prepared = 0;
+            x->prepared = dplur ? 1 : 0;
             return CSU_OK;
         }
         k_state_out<<<g, BLOCK, 0, x->stream>>>(x->st, x->d_stage, x->d_n2o, nc, nv);
