@@ -315,7 +315,7 @@ static void plan(csu_ctx* x, Arena& a)
            : (x->cfg.sa && x->cfg.time_scheme == CSU_TS_DPLUR && x->cfg.sa_implicit_source) ? carve<double>(a, nc)
                                                                                             : nullptr;
     s.gfix = carve<int2>(a, (size_t)nc * (nv + 1)); // at most one entry per cell and variable (and T)
-    s.gfix_n = carve<unsigned>(a, 2);
+    s.gfix_n = carve<unsigned>(a, 1);
     if (!x->is_pack) {
         x->d_n2o = carve<int>(a, nc);
         x->d_stage = carve<double>(a, (size_t)nv * nc);
@@ -931,9 +931,11 @@ static void launch_grad_lsq(csu_ctx* x)
     case 0: k_grad<MODEL, DBG, 0><<<x->gb_c, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st); break;
     case 1: k_grad<MODEL, DBG, 1><<<x->gb_c, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st); break;
     default:
-        // the rare components left undecided by the FP64 paths are finished by k_grad_fix
+        // the rare components left undecided by the FP64 paths are finished by k_grad_fix: grid-stride over a
+        // list whose length only the device knows, two blocks per SM (strongly stretched cells, as beside a
+        // wall at y+ < 1, leave thousands of entries; an empty list costs one short launch)
         k_grad<MODEL, DBG, 2><<<x->gb_c, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st);
-        k_grad_fix<MODEL><<<1, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st);
+        k_grad_fix<MODEL><<<2 * x->sm_count, BLOCK, 0, x->stream>>>(x->d_prm, x->mesh, x->st);
         x->launches++;
         break;
     }

@@ -149,8 +149,8 @@ struct State {
     unsigned long long* lsq_x87;              // running count of gradient slots left to the integer x87 model
     double* dQ;                               // SST LU-SGS: source Jacobians [6][cell] (sst_source_jacobians)
     int2* gfix;                               // gradient variables left to k_grad_fix: (cell, var | mask << 8)
-    unsigned* gfix_n;                         // [0] entries in gfix, [1] k_grad_fix blocks done (both reset
-                                              // by the last block of k_grad_fix)
+    unsigned* gfix_n;                         // entries in gfix (k_grad appends, k_grad_fix reads, the k_flux
+                                              // that follows empties it)
 };
 
 // ---------------------------------------------------------------- small helpers

@@ -209,7 +209,7 @@ __global__ void __launch_bounds__(BLOCK) k_minmax(const Prm* __restrict__ P, con
 }
 
 template <int MODEL, bool DBG, int LSQ>
-__global__ void __launch_bounds__(BLOCK, 3) k_grad(const Prm* __restrict__ P, const __grid_constant__ Mesh m,
+__global__ void __launch_bounds__(BLOCK, MODEL == 0 ? 3 : 2) k_grad(const Prm* __restrict__ P, const __grid_constant__ Mesh m,
                                                 const __grid_constant__ State s)
 {
     constexpr int NV = Model<MODEL>::NV, NP = Model<MODEL>::NP;
@@ -441,8 +441,8 @@ __global__ void __launch_bounds__(BLOCK, 3) k_grad(const Prm* __restrict__ P, co
 // k_grad_fix: the gradient components neither k_grad's certified solve nor its exact x87 numerator could
 // decide, entry (cell, variable kk (NV: temperature), mask of x / y): both components of the variable with
 // the integer x87 model (lsq_slot_x87), the undecided ones taken from it, then the variable's limiter
-// (limiterCalc) from the final gradient, as k_grad computes it. Grid-stride over the entries; the last block
-// to finish empties the list for the next gradient launch.
+// (limiterCalc) from the final gradient, as k_grad computes it. Grid-stride over the entries; k_flux, which
+// always follows, empties the list for the next gradient launch.
 // ------------------------------------------------------------------------------------------------
 template <int MODEL>
 __global__ void __launch_bounds__(BLOCK) k_grad_fix(const Prm* __restrict__ P, const __grid_constant__ Mesh m,
@@ -482,15 +482,6 @@ __global__ void __launch_bounds__(BLOCK) k_grad_fix(const Prm* __restrict__ P, c
             }
             if (kk < 4) reinterpret_cast<double*>(s.PH4 + c)[kk] = phi;
             else s.PHx[(size_t)(kk - 4) * nc + c] = phi;
-        }
-    }
-    // every block read the count above before it counts itself done
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        if (atomicAdd(s.gfix_n + 1, 1u) == gridDim.x - 1) {
-            s.gfix_n[0] = 0;
-            s.gfix_n[1] = 0;
         }
     }
 }
@@ -734,6 +725,8 @@ __global__ void __launch_bounds__(FB) k_flux(const Prm* __restrict__ P, const __
 {
     constexpr int NV = Model<MODEL>::NV, NP = Model<MODEL>::NP;
     const int nc = m.nc;
+    // k_grad_fix (always launched just before) has read its list: empty it for the next gradient launch
+    if (blockIdx.x == 0 && threadIdx.x == 0 && s.gfix_n) *s.gfix_n = 0;
     if ((int)blockIdx.x < nbi) {
         int f = blockIdx.x * FB + threadIdx.x;
         if (f >= m.nf) return;
@@ -766,6 +759,8 @@ __global__ void __launch_bounds__(FB) k_flux_st(const Prm* __restrict__ P, const
                                                 const __grid_constant__ State s, int nbi, const int* wall_rank,
                                                 int coef)
 {
+    // k_grad_fix (always launched just before) has read its list: empty it for the next gradient launch
+    if (blockIdx.x == 0 && threadIdx.x == 0 && s.gfix_n) *s.gfix_n = 0;
     if ((int)blockIdx.x >= nbi) {
         const int b = (blockIdx.x - nbi) * FB + threadIdx.x;
         if (b < m.nb) boundary_face<MODEL>(P, m, s, b, wall_rank, coef);
@@ -1160,7 +1155,7 @@ __global__ void __launch_bounds__(BLOCK) k_impl(const Prm* __restrict__ P, const
 // the cells of cell blocks [0, gb).
 // ------------------------------------------------------------------------------------------------
 template <int MODEL>
-__global__ void __launch_bounds__(BLOCK, 3) k_blocks(const Prm* __restrict__ P, const __grid_constant__ Mesh m,
+__global__ void __launch_bounds__(BLOCK, MODEL == 0 ? 3 : 2) k_blocks(const Prm* __restrict__ P, const __grid_constant__ Mesh m,
                                                   const __grid_constant__ State s, int gb)
 {
     constexpr int NV = Model<MODEL>::NV, NP = Model<MODEL>::NP;
