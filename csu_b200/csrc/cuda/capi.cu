@@ -141,7 +141,7 @@ struct csu_ctx {
     cudaStream_t own_stream = nullptr;
     // DPLUR blocks run on a side stream, forked from and joined back to the engine stream
     cudaStream_t side = nullptr;
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_grad = nullptr;
     // DPLUR graph capture: iterations in the graph being captured and the next one's index; an iteration's
     // k_finalize left to run on the side stream beside the next iteration's gradients and fluxes, with the
     // face-coefficient buffer it sums
@@ -495,6 +495,7 @@ static void fill_params_from(const csu_config& c, const csu_layout& L, Prm& p)
     p.blk32 = c.implicit_fp32;
     p.sa_isrc = c.sa && c.time_scheme == CSU_TS_DPLUR && c.sa_implicit_source;
     p.defer_fin = c.time_scheme == CSU_TS_DPLUR;
+    p.mit_early = c.sa && c.time_scheme == CSU_TS_DPLUR;
     p.implicit_local_dt = c.implicit_local_dt;
     p.cfl_ramp_iters = c.cfl_ramp_iters;
     p.cfl_max = c.cfl_ramp_iters > 0 ? c.cfl_max : c.cfl;
@@ -640,6 +641,7 @@ static int ctx_setup(csu_ctx* x)
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&x->side, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&x->ev_fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&x->ev_join, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&x->ev_grad, cudaEventDisableTiming);
     x->stream = x->own_stream;
     if (e != cudaSuccess) return cuda_fail(e, "context setup");
     x->gb_c = (x->L.nc + BLOCK - 1) / BLOCK;
@@ -728,6 +730,7 @@ extern "C" void csu_destroy(csu_ctx* x)
     if (x->side) cudaStreamDestroy(x->side);
     if (x->ev_fork) cudaEventDestroy(x->ev_fork);
     if (x->ev_join) cudaEventDestroy(x->ev_join);
+    if (x->ev_grad) cudaEventDestroy(x->ev_grad);
     if (x->arena.base) {
         if (x->is_pack) {
             pack_arena_give(x->device, x->arena.base, x->arena.size);
@@ -1009,7 +1012,9 @@ static void launch_prologue(csu_ctx* x)
 // the caller before the kernels they run beside, which are launched first so that their blocks are dispatched
 // first and k_blocks fills the SMs their last wave leaves idle); the first sweep joins. Timed runs keep them
 // on the engine stream, so each kernel kind's events bracket it alone.
-// The implicit diagonal and step (k_impl without R) go on the same side stream.
+// The implicit diagonal and step (k_impl without R) go on the same side stream. SA first computes the face
+// eddy viscosity the blocks and the diagonal use (k_face_mit); with saImplicitSource its diagonal also needs
+// the gradients, so k_impl waits for ev_grad (recorded after them).
 template <int MODEL>
 static void launch_blocks(csu_ctx* x)
 {
@@ -1017,6 +1022,10 @@ static void launch_blocks(csu_ctx* x)
     if (!x->timing) {
         cudaStreamWaitEvent(x->side, x->ev_fork, 0);
         s = x->side;
+    }
+    if (MODEL == 1 && x->prm.mit_early) {
+        k_face_mit<<<(x->L.nf + BLOCK - 1) / BLOCK, BLOCK, 0, s>>>(x->d_prm, x->mesh, x->st);
+        x->launches++;
     }
     k_blocks<MODEL><<<x->max_ni * x->gb_c, BLOCK, 0, s>>>(x->d_prm, x->mesh, x->st, x->gb_c);
     x->launches++;
@@ -1027,6 +1036,7 @@ static void launch_blocks(csu_ctx* x)
         launch_finalize<MODEL>(x, 1, x->fin_bsel, s);
         x->fin_pending = false;
     }
+    if (MODEL == 1 && x->prm.sa_isrc && !x->timing) cudaStreamWaitEvent(x->side, x->ev_grad, 0);
     k_impl<MODEL, false><<<x->gb_c, BLOCK, 0, s>>>(x->d_prm, x->mesh, x->st);
     x->launches++;
     if (x->timing) tmark(x, KIMPL);
@@ -1123,9 +1133,9 @@ static void launch_iteration(csu_ctx* x)
         tmark(x, KPRIM);
         launch_finalize<MODEL>(x, 1);
     } else {
-        // the SA and SST blocks and diagonal need the face eddy viscosity of k_flux (SST's diagonal also the
-        // gradients, for its source Jacobians); the Euler/laminar ones only the iteration's start state
-        constexpr bool early = MODEL == 0;
+        // the SST blocks and diagonal need the face eddy viscosity of k_flux (and the gradients, for the
+        // source Jacobians); the SA ones only k_face_mit's, the Euler/laminar ones the iteration's start state
+        constexpr bool early = MODEL <= 1;
         const bool grad = c.order == 2 || x->prm.visc;
         // Inside a captured graph an iteration's k_finalize (norms, history row, halt flags, counters) runs on
         // the side stream beside the next iteration's gradients and face fluxes, which test halted_behind;
@@ -1141,6 +1151,7 @@ static void launch_iteration(csu_ctx* x)
             x->fin_pending = false;
         }
         if (grad) launch_grad<MODEL>(x, false);
+        if (MODEL == 1 && x->prm.sa_isrc && !x->timing) cudaEventRecord(x->ev_grad, x->stream);
         snapshot_views(x);
         if (early) launch_blocks<MODEL>(x);
         launch_flux<MODEL>(x, 1 + bsel);

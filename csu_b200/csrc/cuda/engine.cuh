@@ -48,6 +48,8 @@ struct Prm {
     int blk32;          // DPLUR blocks in FP32
     int sa_isrc;        // SA + DPLUR: the source's implicit part in the nt diagonal (dQ holds it per cell)
     int defer_fin;      // DPLUR: an iteration's k_finalize may run beside the next one's gradients and fluxes
+    int mit_early;      // SA + DPLUR: k_face_mit writes the face eddy viscosity (from the primitives alone) for
+                        // the blocks and the diagonal, which then need not wait for k_flux; k_flux skips it
     int implicit_local_dt;
     int cfl_ramp_iters; // CFL ramp (0: constant CFL)
     double cfl_max;

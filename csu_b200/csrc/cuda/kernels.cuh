@@ -644,7 +644,7 @@ __device__ __forceinline__ void interior_face(const Prm& p, const Mesh& m, const
             sa_face_flux(p.gas, p.pr, p.pr_t, p.visc_blazek, g0x, g0y, g1x, g1y, A, B, dd.x, dd.y, m.fL[f], dSx,
                          dSy, fv, &mit);
         s.FV[f] = make_double4(fv[0], fv[1], fv[2], fv[3]);
-        s.MIT[f] = mit;
+        if (!p.mit_early) s.MIT[f] = mit;
     } else if (p.laminar == 1) {
         const double4 a = gx0, b = gy0, cc = gx1, d = gy1;
         double g0x[3] = {a.y, a.z, s.GTx[e.x]}, g0y[3] = {b.y, b.z, s.GTy[e.x]};
@@ -1144,6 +1144,33 @@ __global__ void __launch_bounds__(BLOCK) k_impl(const Prm* __restrict__ P, const
     double v = block_min(lmin);
     if (threadIdx.x == 0 && !(v > bitsd(0x7fefffffffffffffULL))) atomicMin(&sc->dtmin_bits, dbits(v));
     if (WITH_R) partial_norms<MODEL>(s, valid, R);
+}
+
+// ------------------------------------------------------------------------------------------------
+// k_face_mit: the SA face eddy viscosity mu_t = fv1 rho nt of the face means of the two cells' primitives
+// (saBoundaryVisc's interior part, sa.c: the same expressions as sa_face_flux / sacc_face_flux, whose value
+// it equals bit for bit), for the DPLUR blocks and diagonal: it needs no gradient, so they can run beside
+// k_grad and k_flux instead of after them.
+// ------------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(BLOCK) k_face_mit(const Prm* __restrict__ P, const __grid_constant__ Mesh m,
+                                                    const __grid_constant__ State s)
+{
+    const int f = blockIdx.x * BLOCK + threadIdx.x;
+    if (f >= m.nf) return;
+    const int2 e = m.fe[f];
+    const int sid = cell_solve(s, e.x);
+    if (halted(s.sc + sid)) return;
+    const int nc = m.nc;
+    const double4 w0 = s.W4[e.x], w1 = s.W4[e.y];
+    const double r = (w1.x + w0.x) * 0.5;
+    const double T = (s.WT[e.y] + s.WT[e.x]) * 0.5;
+    const double n = (s.Wx[e.y] + s.Wx[e.x]) * 0.5;
+    const double mi_L = sutherland(T);
+    const double n_L = mi_L / r;
+    double fv1, tx, ty;
+    sa_face(n, n_L, r, 0.0, 0.0, &fv1, &tx, &ty);
+    s.MIT[f] = fv1 * r * n;
+    (void)nc;
 }
 
 // ------------------------------------------------------------------------------------------------
