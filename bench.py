@@ -212,8 +212,14 @@ def serve_summary(n, cells_hi, rate):
     b, p = out["batched"], out["plain"]
     keys = ("solves_per_hour", "converged", "requests", "failed", "p50_s", "p99_s", "makespan_s",
             "cell_updates_per_s")
+    def ratio(x, y):
+        return x / y if x and y else None
+
     return {"metric": "converged solves/hr", "unit": "solves/hr",
-            "vs_plain_fp64": b["solves_per_hour"] / p["solves_per_hour"] if p["solves_per_hour"] else None,
+            "vs_plain_fp64": ratio(b["solves_per_hour"], p["solves_per_hour"]),
+            # time-to-converge of the plain arm over the batched arm's (higher is better for the batched arm)
+            "p50_plain_over_batched": ratio(p["p50_s"], b["p50_s"]),
+            "p99_plain_over_batched": ratio(p["p99_s"], b["p99_s"]),
             "batched_mixed": {k: b[k] for k in keys}, "plain_fp64": {k: p[k] for k in keys},
             "state_diff_rel": out["state_diff_rel"], "force_coef_diff_rel": out["coef_diff_rel"],
             "workload": out["workload"], "wall_s": time.perf_counter() - t0}
