@@ -723,8 +723,6 @@ __global__ void __launch_bounds__(FB) k_flux(const Prm* __restrict__ P, const __
                                              const __grid_constant__ State s, int nbi, const int* wall_rank,
                                              int coef)
 {
-    constexpr int NV = Model<MODEL>::NV, NP = Model<MODEL>::NP;
-    const int nc = m.nc;
     // k_grad_fix (always launched just before) has read its list: empty it for the next gradient launch
     if (blockIdx.x == 0 && threadIdx.x == 0 && s.gfix_n) *s.gfix_n = 0;
     if ((int)blockIdx.x < nbi) {
