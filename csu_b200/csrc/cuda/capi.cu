@@ -1047,10 +1047,14 @@ template <int MODEL, int SB>
 static void launch_sweep_sb(csu_ctx* x, int m, int n)
 {
     if (m == 0) {
-        auto* k = m == n - 1 ? k_sweep<MODEL, true, true, SB> : k_sweep<MODEL, false, true, SB>;
+        auto* k = x->cfg.implicit_fp32
+                      ? (m == n - 1 ? k_sweep<MODEL, true, true, SB, true> : k_sweep<MODEL, false, true, SB, true>)
+                      : (m == n - 1 ? k_sweep<MODEL, true, true, SB, false> : k_sweep<MODEL, false, true, SB, false>);
         k<<<x->gb_c * (BLOCK / SB), SB, 0, x->stream>>>(x->d_prm, x->mesh, x->st, m, x->xcur);
     } else {
-        auto* k = m == n - 1 ? k_sweep<MODEL, true, false, SB> : k_sweep<MODEL, false, false, SB>;
+        auto* k = x->cfg.implicit_fp32
+                      ? (m == n - 1 ? k_sweep<MODEL, true, false, SB, true> : k_sweep<MODEL, false, false, SB, true>)
+                      : (m == n - 1 ? k_sweep<MODEL, true, false, SB, false> : k_sweep<MODEL, false, false, SB, false>);
         k<<<x->gb_c * (BLOCK / SB), SB, 0, x->stream>>>(x->d_prm, x->mesh, x->st, m, x->xcur);
     }
 }
@@ -1353,9 +1357,18 @@ static int time_sweep_shape(csu_ctx* x, int sb, int reps, cudaEvent_t e0, cudaEv
                          sizeof(unsigned long long), x->nsolve, cudaMemcpyHostToDevice, x->stream));
     auto launch = [&]() {
         switch (sb) {
-        case 64: k_sweep<MODEL, false, false, 64><<<x->gb_c * (BLOCK / 64), 64, 0, x->stream>>>(x->d_prm, x->mesh, x->st, slot, x->xcur); break;
-        case 256: k_sweep<MODEL, false, false, 256><<<x->gb_c, 256, 0, x->stream>>>(x->d_prm, x->mesh, x->st, slot, x->xcur); break;
-        default: k_sweep<MODEL, false, false, 128><<<x->gb_c * 2, 128, 0, x->stream>>>(x->d_prm, x->mesh, x->st, slot, x->xcur); break;
+        case 64:
+            (x->cfg.implicit_fp32 ? k_sweep<MODEL, false, false, 64, true> : k_sweep<MODEL, false, false, 64, false>)
+                <<<x->gb_c * (BLOCK / 64), 64, 0, x->stream>>>(x->d_prm, x->mesh, x->st, slot, x->xcur);
+            break;
+        case 256:
+            (x->cfg.implicit_fp32 ? k_sweep<MODEL, false, false, 256, true> : k_sweep<MODEL, false, false, 256, false>)
+                <<<x->gb_c, 256, 0, x->stream>>>(x->d_prm, x->mesh, x->st, slot, x->xcur);
+            break;
+        default:
+            (x->cfg.implicit_fp32 ? k_sweep<MODEL, false, false, 128, true> : k_sweep<MODEL, false, false, 128, false>)
+                <<<x->gb_c * 2, 128, 0, x->stream>>>(x->d_prm, x->mesh, x->st, slot, x->xcur);
+            break;
         }
     };
     launch();

@@ -1275,7 +1275,7 @@ __global__ void __launch_bounds__(BLOCK, MODEL == 0 ? 3 : 2) k_blocks(const Prm*
 // the cell's residual R from the face fluxes (as k_impl does), stores it for the later sweeps and writes
 // the block's partial norms.
 // ------------------------------------------------------------------------------------------------
-template <int MODEL, bool LAST, bool FIRST, int SB>
+template <int MODEL, bool LAST, bool FIRST, int SB, bool F32>
 __global__ void __launch_bounds__(SB) k_sweep(const Prm* __restrict__ P, const __grid_constant__ Mesh m,
                                               const __grid_constant__ State s, int sweep, int cur)
 {
@@ -1356,19 +1356,34 @@ __global__ void __launch_bounds__(SB) k_sweep(const Prm* __restrict__ P, const _
                 for (int k = 4; k < NV; k++) xb[k] = xox[(size_t)(k - 4) * nc + nb];
                 const size_t base = (size_t)j * NV * NV * nc + c;
                 const bool use = j < ni;
-                double A[NV * NV];
-                if (p.blk32) {
+                if constexpr (F32) {
+                    // FP32 blocks kept as floats until they are used: fewer registers, more cells in flight
+                    float Af[NV * NV];
 #pragma unroll
-                    for (int q = 0; q < NV * NV; q++) A[q] = (double)s.blocks32[base + (size_t)q * nc];
+                    for (int q = 0; q < NV * NV; q++) Af[q] = s.blocks32[base + (size_t)q * nc];
+                    if (use) {
+#pragma unroll
+                        for (int kk = 0; kk < NV; kk++)
+#pragma unroll
+                            for (int nn = 0; nn < NV; nn++) y[kk] += (double)Af[kk * NV + nn] * xb[nn];
+                    }
                 } else {
+                    // FP64 blocks (the FP32 branch stays for contexts launched without F32: as compiled with
+                    // it, the FP64 sweep keeps more of its loads in flight than an FP64-only build does)
+                    double A[NV * NV];
+                    if (p.blk32) {
 #pragma unroll
-                    for (int q = 0; q < NV * NV; q++) A[q] = s.blocks[base + (size_t)q * nc];
-                }
-                if (use) {
+                        for (int q = 0; q < NV * NV; q++) A[q] = (double)s.blocks32[base + (size_t)q * nc];
+                    } else {
 #pragma unroll
-                    for (int kk = 0; kk < NV; kk++)
+                        for (int q = 0; q < NV * NV; q++) A[q] = s.blocks[base + (size_t)q * nc];
+                    }
+                    if (use) {
 #pragma unroll
-                        for (int nn = 0; nn < NV; nn++) y[kk] += A[kk * NV + nn] * xb[nn];
+                        for (int kk = 0; kk < NV; kk++)
+#pragma unroll
+                            for (int nn = 0; nn < NV; nn++) y[kk] += A[kk * NV + nn] * xb[nn];
+                    }
                 }
             }
             const double w = 2. / 3.;
