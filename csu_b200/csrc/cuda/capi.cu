@@ -128,8 +128,8 @@ struct csu_ctx {
     // Nlinear flips it every iteration); captured on first use, kept until the launch sequence changes
     cudaGraphExec_t graphs[4][2] = {};
     long long graph_launches[4][2] = {};
-    // L2 residency of the DPLUR blocks: the sweeps of an iteration read them again and again, and they fit in
-    // L2 on B200; the window is set on the kernel nodes of the captured iteration graphs
+    // L2 residency of the DPLUR blocks when they fit in the persisting part of L2 (plan_l2_window); the window
+    // is set on the kernel nodes of the captured iteration graphs
     cudaAccessPolicyWindow l2win = {};
     Scalars* h_sc = nullptr;   // pinned: solve 0's scalars, read back once at the end of csu_iterate
     int* h_flags = nullptr;    // pinned: halt flags (status, done) of two chunks in flight
@@ -1229,9 +1229,12 @@ static int ensure_hist(csu_ctx* x, int n)
     return write_scalars_n(x, hs.data(), x->nsolve);
 }
 
-// The DPLUR blocks (written once per iteration, read by every sweep) as a persisting L2 window: as much of
-// them as the device lets persist (cudaDevAttrMaxPersistingL2CacheSize), the rest streaming. Only a cache
-// policy: no result depends on it. CSU_L2_PERSIST=0 leaves the L2 alone.
+// The DPLUR blocks (written once per iteration, read by every sweep) as a persisting L2 window, when all of
+// them fit in the part of L2 the device lets persist (cudaDevAttrMaxPersistingL2CacheSize): the bench's 61 MB
+// of FP64 blocks, sweep 19.9 -> 18.9 us. Blocks larger than that are left alone: persisting a fraction of
+// them kept that much L2 from the other kernels and cost more than it saved (a 400k-cell laminar FP64 solve
+// with 205 MB of blocks: 1.16 ms per iteration without the window, 1.41 ms with 40 % of the blocks
+// persisting). Only a cache policy: no result depends on it. CSU_L2_PERSIST=0 leaves the L2 alone.
 static void plan_l2_window(csu_ctx* x)
 {
     x->l2win = cudaAccessPolicyWindow{};
@@ -1247,6 +1250,7 @@ static void plan_l2_window(csu_ctx* x)
         cudaGetLastError();
         return;
     }
+    if (bytes > (size_t)max_persist || bytes > (size_t)max_window) return;
     size_t cur = 0;
     cudaDeviceGetLimit(&cur, cudaLimitPersistingL2CacheSize);
     const size_t want = std::min(bytes, (size_t)max_persist);
