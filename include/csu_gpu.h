@@ -158,7 +158,11 @@ int csu_run_case(const char* wd, int verbose);
 int csu_create(const csu_mesh_desc* mesh, const csu_config* cfg, csu_ctx** out);
 void csu_destroy(csu_ctx* ctx);
 
-/* Upload/download the conserved state, [var][cell] in reference cell order. */
+/* Upload/download the conserved state, [var][cell] in reference cell order (one copy of the caller's
+ * array each way, a DMA when it is pinned; the renumbering runs on the device; both return once the copy
+ * is done). A new state restarts the solve's scalars (history rows, residual-drop reference, halt flags)
+ * for the next csu_iterate; a DPLUR context also computes the state's primitives (solverCalcPrimitive's
+ * clamps written back, solver.c:1153-1220) during the upload. */
 int csu_set_state(csu_ctx* ctx, const double* U);
 int csu_get_state(csu_ctx* ctx, double* U);
 /* Same with the reference's row pointers: U[k][i] (solver->U). */
